@@ -1,0 +1,452 @@
+// adgpu_device.cuh -- device-side data layout and scorer of the B200 engine.
+//
+// A pose (one genotype of one ligand) is scored by a "pose group" of TPP
+// threads (32: one warp; 64/128: several warps joined by a named barrier).
+// Per-ligand constant tables are repacked once on the host (adgpu_tables.cpp)
+// into the LigDev layout below; the grid maps are re-laid out so that the 8
+// corners of one cell of one map are 32 contiguous, 32-byte-aligned bytes,
+// and all maps of a cell sit together (e, d first, then the type maps), so an
+// atom's three trilinear lookups are six 128-bit loads from one cell record.
+//
+// Arithmetic follows the reference scorer operation by operation
+// (gpu_calc_energy, cuda/calcenergy.cu:114-453; gpu_calc_energrad,
+// cuda/calcMergeEneGra.cu:48-900), including its fixed-point gradient
+// accumulation (terms rounded to 1/1024 and clamped to +-8, cuda/GpuData.h:31-35),
+// so results agree with the reference to float rounding of single terms.
+#pragma once
+#include <cstdint>
+#include <cfloat>
+#include <cuda_runtime.h>
+
+namespace adgpu {
+
+// ---- constants (common/calcenergy_basic.h, common/defines.h, cuda/GpuData.h) ----
+constexpr float kDegToRad = 0.0174533f;
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kPiTimes2 = 2.0f * kPi;
+constexpr float kInvPiTimes2 = 1.0f / kPiTimes2;
+constexpr float kTermScale = 1024.0f;
+constexpr float kOneOverTermScale = 1.0f / 1024.0f;
+constexpr float kMaxTerm = 8192.0f;
+constexpr float kMaxEnergy = FLT_MAX / 100.0f;
+constexpr float kInfinitesimalRadian = 1E-3f;
+constexpr float kInvInfinitesimalRadian = 1.0f / kInfinitesimalRadian;
+constexpr float kScAngstromRadian = 1.0f / (kDegToRad * kDegToRad);
+constexpr float kOutOfGridPenalty = 16777216.0f;
+constexpr int kOutOfGridForce = 16777216;
+constexpr int kMaxAtoms = 256;
+constexpr int kMaxGenes = 63;
+constexpr int kGenotypeStride = 64;
+
+// ---- repacked per-ligand tables --------------------------------------------------
+// Pair record: the type-pair parameters and the charge/desolvation prefactors
+// of one intramolecular contributor, so the pair loop reads 32 contiguous bytes.
+struct __align__(16) PairRec {
+	float ac, bd, reqm, dsolv_pref;   // VWpars_AC, VWpars_BD, reqm_AB, (S1+qasp|q1|)V2+(S2+qasp|q2|)V1
+	float qq;                         // coeff_elec*q1*q2
+	float vbond;                      // G for a CG-G0 pair, else 0
+	uint32_t ij;                      // atom1 | atom2<<8 | m<<16 | n<<24
+	uint32_t pad;
+};
+
+struct LigDev {
+	// sizes
+	int natoms, nlig, ngenes, ntors, npairs, ntoritems;
+	int map_e;                   // index of the e map in the cell record (0)
+	// grid
+	int gx, gy, gz;              // grid points per axis
+	int cells_x, cells_xy;       // cells per row / plane
+	int rec_floats;              // floats per cell record = 8*(num_maps)
+	float spacing, inv_spacing;
+	float coeff_desolv, elec_min_distance, half_smooth;
+	// tables (device pointers)
+	const float4* atom_xyzq;     // reference coordinates (grid units) + charge
+	const uint32_t* atom_info;   // bits 0-7 map-record slot, bit 8 ignore_inter, bit 9 general rotation, bits 16-31 chain start
+	const uint8_t* chain_len;    // torsion rotations per atom
+	const uint8_t* chain;        // torsion ids, per atom, in application order
+	const float4* tors_uv;       // rotatable bond unit vectors
+	const float4* tors_mv;       // rotatable bond moving vectors
+	const int2* tors_ends;       // rotatable bond atom pair
+	const uint32_t* tor_items;   // (torsion<<8 | atom) per rotating atom, grouped by torsion
+	const PairRec* pairs;
+	const float* grid;           // cell records, 32-byte aligned
+};
+
+// ---- math helpers (cuda/calcenergy.cu:31-109) ----------------------------------
+__device__ __forceinline__ float fmod_pi2(float x) { return x - (float)(int)(kInvPiTimes2 * x) * kPiTimes2; }
+
+// The reference's acos fit (cuda/calcenergy.cu:48-65); the orientation
+// gradient is defined through it, so it is kept term for term.
+__device__ __forceinline__ float fast_acos(float cosine)
+{
+	const float a = 9.78056e-05f, b = -0.00104588f, c = 0.00418716f, d = -0.00314347f;
+	const float e = 2.74084f, f = 0.370388f, o = -(a + b + c + d);
+	float x = fabsf(cosine);
+	float x2 = x * x, x3 = x2 * x, x4 = x3 * x;
+	float ac = (((o * x4 + a) * x3 + b) * x2 + c) * x + d
+	           + e * sqrtf(2.0f - sqrtf(2.0f + 2.0f * x)) - f * sqrtf(2.0f - 2.0f * x);
+	return copysignf(ac, cosine) + (float)(cosine < 0.0f) * kPi;
+}
+
+__device__ __forceinline__ float3 cross3(float3 u, float3 v)
+{
+	return make_float3(u.y * v.z - v.y * u.z, v.x * u.z - u.x * v.z, u.x * v.y - v.x * u.y);
+}
+
+__device__ __forceinline__ float4 qmul(float4 a, float4 b)
+{
+	return make_float4(a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y,
+	                   a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+	                   a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w,
+	                   a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z);
+}
+
+// quaternion_rotate, cuda/calcenergy.cu:95-109
+__device__ __forceinline__ float3 qrot(float3 v, float4 q)
+{
+	float3 qv = make_float3(q.x, q.y, q.z);
+	float3 z = cross3(qv, v);
+	z.x *= 2.0f; z.y *= 2.0f; z.z *= 2.0f;
+	float3 c = cross3(qv, z);
+	return make_float3(v.x + z.x * q.w + c.x, v.y + z.y * q.w + c.y, v.z + z.z * q.w + c.z);
+}
+
+__device__ __forceinline__ int quant(float v)
+{
+	return __float2int_rn(fminf(kMaxTerm, fmaxf(-kMaxTerm, kTermScale * v)));
+}
+
+// ---- PRNG: the reference's per-thread LCG (cuda/auxiliary_genetic.cu:29-79) ------
+__device__ __forceinline__ uint32_t lcg_next(uint32_t& s) { s = 1103515245u * s + 12345u; return s; }
+__device__ __forceinline__ float lcg_float(uint32_t& s) { return ((float)lcg_next(s) / 4294967296.0f) * 0.999999f; }
+__device__ __forceinline__ void map_angle(float& a)
+{
+	while (a >= 360.0f) a -= 360.0f;
+	while (a < 0.0f) a += 360.0f;
+}
+
+// ---- pose group ------------------------------------------------------------------
+// TPP threads scoring one pose.  TPP == 32 is warp-synchronous; larger groups
+// sync with a named barrier (id 1 + group index within the CTA).
+template <int TPP>
+struct Group {
+	int rank;          // 0..TPP-1
+	int bar_id;        // named barrier for TPP > 32
+	float* red;        // TPP/32 * 8 floats of scratch for cross-warp reductions
+
+	__device__ __forceinline__ void sync() const
+	{
+		if constexpr (TPP == 32) __syncwarp();
+		else asm volatile("bar.sync %0, %1;" :: "r"(bar_id), "r"(TPP) : "memory");
+	}
+
+	__device__ __forceinline__ float sum(float v) const
+	{
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+		if constexpr (TPP == 32) {
+			return v;
+		} else {
+			const int w = rank >> 5;
+			sync();
+			if ((rank & 31) == 0) red[w] = v;
+			sync();
+			float s = 0.0f;
+#pragma unroll
+			for (int i = 0; i < TPP / 32; i++) s += red[i];
+			return s;
+		}
+	}
+
+	// Six sums in one pass (torque x,y,z and force x,y,z).
+	__device__ __forceinline__ void sum6(float* v) const
+	{
+#pragma unroll
+		for (int k = 0; k < 6; k++) {
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+		}
+		if constexpr (TPP != 32) {
+			const int w = rank >> 5;
+			sync();
+			if ((rank & 31) == 0)
+				for (int k = 0; k < 6; k++) red[w * 8 + k] = v[k];
+			sync();
+			for (int k = 0; k < 6; k++) {
+				float s = 0.0f;
+				for (int i = 0; i < TPP / 32; i++) s += red[i * 8 + k];
+				v[k] = s;
+			}
+		}
+	}
+};
+
+// ---- per-pose shared-memory scratch -------------------------------------------------
+// Layout (floats/ints, natoms rounded up to a multiple of 4):
+//   x, y, z [N]; fx, fy, fz [N] (int); tq [ntors] float4; gg [64] int
+struct PoseSmem {
+	float* x; float* y; float* z;
+	int* fx; int* fy; int* fz;
+	float4* tq;
+	int* gg;
+};
+
+__host__ __device__ inline int pose_smem_bytes(int natoms, int ntors)
+{
+	int n4 = (natoms + 3) & ~3;
+	return (6 * n4) * 4 + ntors * 16 + 64 * 4;
+}
+
+__device__ __forceinline__ PoseSmem carve_pose(char* base, int natoms, int ntors)
+{
+	PoseSmem s;
+	int n4 = (natoms + 3) & ~3;
+	float* f = reinterpret_cast<float*>(base);
+	s.tq = reinterpret_cast<float4*>(f);          // 16-byte aligned first
+	f += ntors * 4;
+	s.x = f; s.y = f + n4; s.z = f + 2 * n4;
+	s.fx = reinterpret_cast<int*>(f + 3 * n4);
+	s.fy = s.fx + n4; s.fz = s.fy + n4;
+	s.gg = s.fz + n4;
+	return s;
+}
+
+// Genotype-derived general rotation (cuda/calcMergeEneGra.cu:92-120).
+struct GenRot {
+	float4 q;       // unit quaternion
+	float3 mv;      // translation (grid units)
+	float sin_theta, sin_half, is_theta_gt_pi;
+};
+
+__device__ __forceinline__ GenRot genrot_of(const float* g, bool has_ligand)
+{
+	GenRot r;
+	r.q = make_float4(0.f, 0.f, 0.f, 1.f);
+	r.mv = make_float3(0.f, 0.f, 0.f);
+	r.sin_theta = 0.f; r.sin_half = 0.f; r.is_theta_gt_pi = 1.f;
+	if (has_ligand) {
+		float phi = g[3] * kDegToRad, theta = g[4] * kDegToRad, rotangle = g[5] * kDegToRad;
+		r.mv = make_float3(g[0], g[1], g[2]);
+		float st, ct, sp, cp, sh, ch;
+		sincosf(theta, &st, &ct);
+		sincosf(phi, &sp, &cp);
+		sincosf(rotangle * 0.5f, &sh, &ch);
+		r.q = make_float4(sh * st * cp, sh * st * sp, sh * ct, ch);
+		r.sin_theta = st; r.sin_half = sh;
+		r.is_theta_gt_pi = 1.0f - 2.0f * (float)(st < 0.0f);
+	}
+	return r;
+}
+
+// ---- the scorer -----------------------------------------------------------------------
+// Scores genotype g (shared memory, read-only here).  Returns the energy (same
+// value in every thread of the group).  With GRAD, writes dE/dgene to
+// grad[0..ngenes) (shared memory).  Leaves the pose coordinates in S.
+template <int TPP, bool GRAD>
+__device__ float score_pose(const LigDev& L, const float* __restrict__ g, float* __restrict__ grad,
+                           const PoseSmem& S, const Group<TPP>& G)
+{
+	const int rank = G.rank;
+	// 1. torsion quaternions (cuda/calcMergeEneGra.cu:160-175, computed once per torsion)
+	for (int k = rank; k < L.ntors; k += TPP) {
+		float s, c;
+		sincosf(g[6 + k] * kDegToRad * 0.5f, &s, &c);
+		float4 u = L.tors_uv[k];
+		S.tq[k] = make_float4(s * u.x, s * u.y, s * u.z, c);
+	}
+	if (GRAD)
+		for (int k = rank; k < L.ngenes; k += TPP) S.gg[k] = 0;
+	const GenRot gr = genrot_of(g, L.nlig > 0);
+	G.sync();
+
+	// 2. pose: each atom applies its own torsion chain, then the general rotation
+	//    (the per-atom order the reference's rotation list encodes, cuda/calcMergeEneGra.cu:131-190)
+	for (int a = rank; a < L.natoms; a += TPP) {
+		float4 r4 = L.atom_xyzq[a];
+		float3 p = make_float3(r4.x, r4.y, r4.z);
+		uint32_t info = L.atom_info[a];
+		int cs = info >> 16, cl = L.chain_len[a];
+		for (int i = 0; i < cl; i++) {
+			int k = L.chain[cs + i];
+			float4 m4 = L.tors_mv[k];
+			float3 m = make_float3(m4.x, m4.y, m4.z);
+			p.x -= m.x; p.y -= m.y; p.z -= m.z;
+			p = qrot(p, S.tq[k]);
+			p.x += m.x; p.y += m.y; p.z += m.z;
+		}
+		if ((info & 0x200u) && a < L.nlig) {
+			p = qrot(p, gr.q);
+			p.x += gr.mv.x; p.y += gr.mv.y; p.z += gr.mv.z;
+		}
+		S.x[a] = p.x; S.y[a] = p.y; S.z[a] = p.z;
+	}
+	G.sync();
+
+	// 3. intermolecular: trilinear interpolation of the type, e and d maps
+	//    (cuda/calcMergeEneGra.cu:195-413)
+	float e_acc = 0.0f;
+	for (int a = rank; a < L.natoms; a += TPP) {
+		uint32_t info = L.atom_info[a];
+		int fx = 0, fy = 0, fz = 0;
+		if (!(info & 0x100u)) {
+			float x = S.x[a], y = S.y[a], z = S.z[a];
+			float q = L.atom_xyzq[a].w;
+			if (x < 0.f || y < 0.f || z < 0.f || x >= (float)(L.gx - 1) || y >= (float)(L.gy - 1) || z >= (float)(L.gz - 1)) {
+				e_acc += kOutOfGridPenalty;
+				fx = fy = fz = kOutOfGridForce;
+			} else {
+				float xl = floorf(x), yl = floorf(y), zl = floorf(z);
+				int cell = (int)xl + (int)yl * L.cells_x + (int)zl * L.cells_xy;
+				const float4* rec = reinterpret_cast<const float4*>(L.grid + (size_t)cell * L.rec_floats);
+				float dx = x - xl, omdx = 1.0f - dx, dy = y - yl, omdy = 1.0f - dy, dz = z - zl, omdz = 1.0f - dz;
+				float w0 = omdx * omdy * omdz, w1 = omdx * dy * omdz, w2 = omdx * omdy * dz, w3 = omdx * dy * dz;
+				float w4 = dx * omdy * omdz, w5 = dx * dy * omdz, w6 = dx * omdy * dz, w7 = dx * dy * dz;
+				int slot = info & 0xFFu;
+				float4 t0 = __ldg(rec + 2 * slot), t1 = __ldg(rec + 2 * slot + 1);
+				float4 e0 = __ldg(rec + 0), e1 = __ldg(rec + 1);
+				float4 d0 = __ldg(rec + 2), d1 = __ldg(rec + 3);
+				float vt = t0.x * w0 + t0.y * w1 + t0.z * w2 + t0.w * w3 + t1.x * w4 + t1.y * w5 + t1.z * w6 + t1.w * w7;
+				float ve = e0.x * w0 + e0.y * w1 + e0.z * w2 + e0.w * w3 + e1.x * w4 + e1.y * w5 + e1.z * w6 + e1.w * w7;
+				float vd = d0.x * w0 + d0.y * w1 + d0.z * w2 + d0.w * w3 + d1.x * w4 + d1.y * w5 + d1.z * w6 + d1.w * w7;
+				e_acc += vt;
+				e_acc += q * ve;
+				e_acc += fabsf(q) * vd;
+				if (GRAD) {
+					// corners: .x .y .z .w of rec0 = 000 010 001 011 ; of rec1 = 100 110 101 111
+#define ADGPU_GX(c0, c1) (omdz * (omdy * (c1.x - c0.x) + dy * (c1.y - c0.y)) + dz * (omdy * (c1.z - c0.z) + dy * (c1.w - c0.w)))
+#define ADGPU_GY(c0, c1) (omdz * (omdx * (c0.y - c0.x) + dx * (c1.y - c1.x)) + dz * (omdx * (c0.w - c0.z) + dx * (c1.w - c1.z)))
+#define ADGPU_GZ(c0, c1) (omdy * (omdx * (c0.z - c0.x) + dx * (c1.z - c1.x)) + dy * (omdx * (c0.w - c0.y) + dx * (c1.w - c1.y)))
+					float inv = L.inv_spacing;
+					float gxx = ADGPU_GX(t0, t1) * inv, gyy = ADGPU_GY(t0, t1) * inv, gzz = ADGPU_GZ(t0, t1) * inv;
+					float q1 = q * inv;
+					gxx += q1 * ADGPU_GX(e0, e1); gyy += q1 * ADGPU_GY(e0, e1); gzz += q1 * ADGPU_GZ(e0, e1);
+					q1 = fabsf(q1);
+					gxx += q1 * ADGPU_GX(d0, d1); gyy += q1 * ADGPU_GY(d0, d1); gzz += q1 * ADGPU_GZ(d0, d1);
+#undef ADGPU_GX
+#undef ADGPU_GY
+#undef ADGPU_GZ
+					fx = quant(gxx); fy = quant(gyy); fz = quant(gzz);
+				}
+			}
+		}
+		if (GRAD) { S.fx[a] = fx; S.fy[a] = fy; S.fz[a] = fz; }
+	}
+	if (GRAD) G.sync();
+
+	// 4. intramolecular pairs (cuda/calcMergeEneGra.cu:418-602)
+	for (int p = rank; p < L.npairs; p += TPP) {
+		const float4* pr = reinterpret_cast<const float4*>(L.pairs + p);
+		float4 A = __ldg(pr), B = __ldg(pr + 1);
+		uint32_t ij = __float_as_uint(B.z);
+		int a1 = ij & 0xFF, a2 = (ij >> 8) & 0xFF, m = (ij >> 16) & 0xFF, n = ij >> 24;
+		float subx = S.x[a1] - S.x[a2], suby = S.y[a1] - S.y[a2], subz = S.z[a1] - S.z[a2];
+		float dist = sqrtf(subx * subx + suby * suby + subz * subz);
+		float r = dist * L.spacing;
+		float pg = B.y;                       // vbond (G for CG-G0 pairs)
+		e_acc += B.y * r;
+		if (r < 8.0f) {
+			float delta = A.z - r, sd;
+			if (fabsf(delta) >= L.half_smooth) sd = r + copysignf(L.half_smooth, delta);
+			else sd = A.z;
+			// integer powers by repeated multiplication: s^(m-n) and s^-m
+			float inv = 1.0f / sd;
+			float rm = 1.0f, rmn = 1.0f;
+			{
+				float b = inv; int e = m;
+				while (e) { if (e & 1) rm *= b; b *= b; e >>= 1; }
+				int k = m - n;
+				if (k >= 0) { b = sd; e = k; } else { b = inv; e = -k; }
+				while (e) { if (e & 1) rmn *= b; b *= b; e >>= 1; }
+			}
+			e_acc += (A.x - rmn * A.y) * rm;
+			if (GRAD) pg += ((float)n * A.y * rmn - (float)m * A.x) * rm * inv;
+		}
+		if (r < 20.48f) {
+			if (r < L.elec_min_distance) r = L.elec_min_distance;
+			float d2 = r * r;
+			float desolv = A.w * (L.coeff_desolv * (12.96f - 0.1063f * d2 * (1.0f - 0.001947f * d2)) /
+			                      (12.96f + d2 * (0.4137f + d2 * (0.00357f + 0.000112f * d2))));
+			float shift = r + 1.26366f;
+			float s2 = shift * shift;
+			float diel = 1.10859f / s2 + 0.010358f;
+			float es = B.x / r;
+			e_acc += diel * es + desolv;
+			if (GRAD) pg += -(es / r) * diel - es * 2.21718f / (s2 * shift) - 0.0771605f * r * desolv;
+		}
+		if (GRAD) {
+			float gdd = -pg / dist;
+			int ix = quant(subx * gdd), iy = quant(suby * gdd), iz = quant(subz * gdd);
+			atomicSub(&S.fx[a1], ix); atomicSub(&S.fy[a1], iy); atomicSub(&S.fz[a1], iz);
+			atomicAdd(&S.fx[a2], ix); atomicAdd(&S.fy[a2], iy); atomicAdd(&S.fz[a2], iz);
+		}
+	}
+	const float energy = G.sum(e_acc);
+	if (!GRAD) return energy;
+	G.sync();
+
+	// 5. torque and total force over the ligand atoms (cuda/calcMergeEneGra.cu:608-661)
+	float red[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+	for (int a = rank; a < L.nlig; a += TPP) {
+		float3 r = make_float3((S.x[a] - gr.mv.x) * L.spacing, (S.y[a] - gr.mv.y) * L.spacing, (S.z[a] - gr.mv.z) * L.spacing);
+		float3 f = make_float3(kOneOverTermScale * (float)S.fx[a], kOneOverTermScale * (float)S.fy[a], kOneOverTermScale * (float)S.fz[a]);
+		red[3] += f.x; red[4] += f.y; red[5] += f.z;
+		float3 t = cross3(r, f);
+		red[0] += t.x; red[1] += t.y; red[2] += t.z;
+	}
+	G.sum6(red);
+	if (rank == 0 && L.nlig > 0) {
+		// translation (:676-689) and orientation (:695-815) genes
+		S.gg[0] = quant(red[3] * L.spacing);
+		S.gg[1] = quant(red[4] * L.spacing);
+		S.gg[2] = quant(red[5] * L.spacing);
+		float tl = norm3df(red[0], red[1], red[2]);
+		float oscale = (tl < kInfinitesimalRadian) ? 1.0f : tl * kInvInfinitesimalRadian;
+		// sin/cos of half the infinitesimal rotation (SIN/COS_HALF_INFINITESIMAL_RADIAN)
+		const float kSinHalfInf = sinf(0.5f * kInfinitesimalRadian), kCosHalfInf = cosf(0.5f * kInfinitesimalRadian);
+		float tscale = (tl < kInfinitesimalRadian) ? 0.5f - tl * tl / 48.0f : kSinHalfInf / tl;
+		float4 qt = make_float4(red[0] * tscale, red[1] * tscale, red[2] * tscale,
+		                        (tl < kInfinitesimalRadian) ? 1.0f - tl * tl * 0.125f : kCosHalfInf);
+		float4 tgt = qmul(qt, gr.q);
+		float cur_phi = fmod_pi2(kPiTimes2 + g[3] * kDegToRad);
+		float cur_theta = fmod_pi2(kPiTimes2 + g[4] * kDegToRad);
+		float cur_rot = fmod_pi2(kPiTimes2 + g[5] * kDegToRad);
+		float tgt_rot = 2.0f * fast_acos(tgt.w);
+		float sin_ang = sqrtf(1.0f - tgt.w * tgt.w);
+		float tgt_theta = kPiTimes2 + gr.is_theta_gt_pi * fast_acos(tgt.z / sin_ang);
+		float tgt_phi = fmod_pi2(atan2f(gr.is_theta_gt_pi * tgt.y, gr.is_theta_gt_pi * tgt.x) + kPiTimes2);
+		float gphi = oscale * (fmod_pi2(tgt_phi - cur_phi + kPi) - kPi);
+		float gth = oscale * (fmod_pi2(tgt_theta - cur_theta + kPi) - kPi);
+		float grot = oscale * (fmod_pi2(tgt_rot - cur_rot + kPi) - kPi);
+		float corr = 4.0f * gr.sin_half * gr.sin_half;
+		S.gg[3] = quant(gphi * gr.sin_theta * gr.sin_theta * corr * kDegToRad);
+		S.gg[4] = quant(gth * corr * kDegToRad);
+		S.gg[5] = quant(grot * kDegToRad);
+	}
+
+	// 6. torsion genes: axis . (r x F) summed over each torsion's rotating atoms (:819-880)
+	for (int it = rank; it < L.ntoritems; it += TPP) {
+		uint32_t item = L.tor_items[it];
+		int k = item >> 8, la = item & 0xFF;
+		int2 ends = L.tors_ends[k];
+		float rx = S.x[ends.x], ry = S.y[ends.x], rz = S.z[ends.x];
+		float ux = S.x[ends.y] - rx, uy = S.y[ends.y] - ry, uz = S.z[ends.y] - rz;
+		float l = rnorm3df(ux, uy, uz);
+		ux *= l; uy *= l; uz *= l;
+		float3 r = make_float3(S.x[la] - rx, S.y[la] - ry, S.z[la] - rz);
+		float3 f = make_float3(kOneOverTermScale * (float)S.fx[la], kOneOverTermScale * (float)S.fy[la], kOneOverTermScale * (float)S.fz[la]);
+		float3 t = cross3(r, f);
+		float on_axis = (ux * t.x + uy * t.y + uz * t.z) * L.spacing;
+		atomicAdd(&S.gg[6 + k], quant(on_axis * kDegToRad));
+	}
+	G.sync();
+	// 7. fixed point -> float, Angstrom/radian scaling of genes >= 3 (:883-899)
+	const float sc = L.spacing * L.spacing * kScAngstromRadian;
+	for (int k = rank; k < L.ngenes; k += TPP) {
+		float v = kOneOverTermScale * (float)S.gg[k];
+		grad[k] = (k >= 3) ? v * sc : v;
+	}
+	G.sync();
+	return energy;
+}
+
+}  // namespace adgpu

@@ -1,0 +1,256 @@
+// adgpu_tables.cu -- repacking of the reference's per-ligand tables into the
+// engine's device layout, and the grid relayout.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+#include "adgpu_tables.h"
+
+namespace adgpu {
+
+__global__ void relayout_grid_kernel(const float* __restrict__ ref, float* __restrict__ out,
+                                     int gx, int gy, int gz, int nmaps, int num_map_atypes);
+
+LigandTables::~LigandTables() { release(); }
+
+void LigandTables::release()
+{
+	if (dmem) cudaFree(dmem);
+	if (dgrid && own_grid) cudaFree(dgrid);
+	dmem = nullptr; dgrid = nullptr; dmem_bytes = 0; dgrid_bytes = 0;
+}
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+size_t cell_grid_bytes(int gx, int gy, int gz, int num_map_atypes)
+{
+	return (size_t)(gx - 1) * (gy - 1) * (gz - 1) * (size_t)(num_map_atypes + 2) * 8 * sizeof(float);
+}
+
+adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii, const uint32_t* pairs,
+                         const adgpu_kc_intra& kin, const int* rotlist, const adgpu_kc_conform& cf,
+                         const int* rotbonds, const int* rotbonds_atoms, const int* nrot, PackedLigand& out)
+{
+	const int N = dp.num_of_atoms, NG = dp.num_of_genes, NT = NG - 6, Q = dp.num_of_intraE_contributors;
+	if (N <= 0 || N > ADGPU_MAX_ATOMS) return fail(ADGPU_ERR_LIMIT, "num_of_atoms out of range 1..256");
+	if (NG < 6 || NG > ADGPU_MAX_GENES) return fail(ADGPU_ERR_LIMIT, "num_of_genes out of range 6..63");
+	if (dp.true_ligand_atoms < 0 || dp.true_ligand_atoms > N) return fail(ADGPU_ERR_ARG, "true_ligand_atoms out of range");
+	if (Q < 0 || Q > ADGPU_MAX_INTRAE) return fail(ADGPU_ERR_LIMIT, "num_of_intraE_contributors out of range");
+	if (dp.num_of_atypes <= 0 || dp.num_of_atypes > ADGPU_MAX_ATYPES) return fail(ADGPU_ERR_LIMIT, "num_of_atypes out of range");
+	if (dp.rotbondlist_length < 0 || dp.rotbondlist_length > ADGPU_MAX_ROTATIONS) return fail(ADGPU_ERR_LIMIT, "rotbondlist_length out of range");
+	if (dp.num_of_map_atypes <= 0 || dp.num_of_map_atypes + 2 > 255) return fail(ADGPU_ERR_LIMIT, "num_of_map_atypes out of range");
+	out = PackedLigand();
+	out.natoms = N; out.nlig = dp.true_ligand_atoms; out.ngenes = NG; out.ntors = NT; out.npairs = Q;
+
+	// per-atom rotation chains from the rotation list: every non-dummy entry of
+	// atom a, in list order (host/src/calcenergy.cpp:387-488 orders them
+	// torsions first, the general rotation last)
+	std::vector<std::vector<uint8_t>> chains(N);
+	std::vector<bool> genrot(N, false);
+	for (int k = 0; k < dp.rotbondlist_length; k++) {
+		int el = rotlist[k];
+		if (el & ADGPU_RLIST_DUMMY_MASK) continue;
+		int a = el & ADGPU_RLIST_ATOMID_MASK;
+		if (a >= N) return fail(ADGPU_ERR_ARG, "rotation list names an atom beyond num_of_atoms");
+		if (el & ADGPU_RLIST_GENROT_MASK) {
+			if (genrot[a]) return fail(ADGPU_ERR_ARG, "rotation list applies the general rotation twice");
+			genrot[a] = true;
+		} else {
+			if (genrot[a]) return fail(ADGPU_ERR_ARG, "rotation list rotates an atom about a torsion after the general rotation");
+			int rb = (el & ADGPU_RLIST_RBONDID_MASK) >> ADGPU_RLIST_RBONDID_SHIFT;
+			if (rb >= NT) return fail(ADGPU_ERR_ARG, "rotation list names a torsion beyond num_of_genes-6");
+			chains[a].push_back((uint8_t)rb);
+		}
+	}
+	// torsion items
+	std::vector<uint32_t> items;
+	for (int k = 0; k < NT; k++) {
+		if (nrot[k] < 0 || nrot[k] > N) return fail(ADGPU_ERR_ARG, "num_rotating_atoms_per_rotbond out of range");
+		if (rotbonds[2 * k] < 0 || rotbonds[2 * k] >= N || rotbonds[2 * k + 1] < 0 || rotbonds[2 * k + 1] >= N)
+			return fail(ADGPU_ERR_ARG, "rotbond atom out of range");
+		for (int c = 0; c < nrot[k]; c++) {
+			int la = rotbonds_atoms[ADGPU_MAX_ATOMS * k + c];
+			if (la < 0 || la >= N) return fail(ADGPU_ERR_ARG, "rotating atom out of range");
+			items.push_back(((uint32_t)k << 8) | (uint32_t)la);
+		}
+	}
+	out.ntoritems = (int)items.size();
+	size_t nchain = 0;
+	for (auto& c : chains) nchain += c.size();
+	if (nchain > 65535) return fail(ADGPU_ERR_LIMIT, "rotation chains too long");
+
+	// layout of the blob
+	size_t o = 0;
+	out.off_atom_xyzq = o; o = align_up(o + (size_t)N * 16, 16);
+	out.off_atom_info = o; o = align_up(o + (size_t)N * 4, 16);
+	out.off_chain_len = o; o = align_up(o + (size_t)N, 16);
+	out.off_chain = o; o = align_up(o + std::max<size_t>(nchain, 1), 16);
+	out.off_tors_uv = o; o = align_up(o + (size_t)std::max(NT, 1) * 16, 16);
+	out.off_tors_mv = o; o = align_up(o + (size_t)std::max(NT, 1) * 16, 16);
+	out.off_tors_ends = o; o = align_up(o + (size_t)std::max(NT, 1) * 8, 16);
+	out.off_tor_items = o; o = align_up(o + std::max<size_t>(items.size(), 1) * 4, 16);
+	out.off_pairs = o; o = align_up(o + (size_t)std::max(Q, 1) * sizeof(PairRec), 16);
+	out.blob.assign(o, 0);
+	uint8_t* B = out.blob.data();
+
+	float4* xyzq = reinterpret_cast<float4*>(B + out.off_atom_xyzq);
+	uint32_t* info = reinterpret_cast<uint32_t*>(B + out.off_atom_info);
+	uint8_t* clen = B + out.off_chain_len;
+	uint8_t* chain = B + out.off_chain;
+	size_t cpos = 0;
+	for (int a = 0; a < N; a++) {
+		xyzq[a] = make_float4(cf.ref_coords_const[3 * a], cf.ref_coords_const[3 * a + 1], cf.ref_coords_const[3 * a + 2],
+		                      ii.atom_charges_const[a]);
+		uint32_t mt = ii.atom_types_map_const[a];
+		bool ignore = ii.ignore_inter_const[a] > 0;
+		if (!ignore && mt >= (uint32_t)dp.num_of_map_atypes) return fail(ADGPU_ERR_ARG, "atom map type out of range");
+		uint32_t slot = ignore ? 0u : (2u + mt);
+		info[a] = slot | (ignore ? 0x100u : 0u) | (genrot[a] ? 0x200u : 0u) | ((uint32_t)cpos << 16);
+		clen[a] = (uint8_t)chains[a].size();
+		for (uint8_t k : chains[a]) chain[cpos++] = k;
+		out.rot_ops += (long)chains[a].size() + (genrot[a] && a < dp.true_ligand_atoms ? 1 : 0);
+		if (ii.atom_types_const[a] >= (uint32_t)dp.num_of_atypes) return fail(ADGPU_ERR_ARG, "atom type out of range");
+	}
+	float4* uv = reinterpret_cast<float4*>(B + out.off_tors_uv);
+	float4* mv = reinterpret_cast<float4*>(B + out.off_tors_mv);
+	int2* ends = reinterpret_cast<int2*>(B + out.off_tors_ends);
+	for (int k = 0; k < NT; k++) {
+		uv[k] = make_float4(cf.rotbonds_unit_vectors_const[3 * k], cf.rotbonds_unit_vectors_const[3 * k + 1], cf.rotbonds_unit_vectors_const[3 * k + 2], 0.f);
+		mv[k] = make_float4(cf.rotbonds_moving_vectors_const[3 * k], cf.rotbonds_moving_vectors_const[3 * k + 1], cf.rotbonds_moving_vectors_const[3 * k + 2], 0.f);
+		ends[k] = make_int2(rotbonds[2 * k], rotbonds[2 * k + 1]);
+	}
+	memcpy(B + out.off_tor_items, items.data(), items.size() * 4);
+	PairRec* pr = reinterpret_cast<PairRec*>(B + out.off_pairs);
+	const int nat = dp.num_of_atypes;
+	for (int p = 0; p < Q; p++) {
+		uint32_t a1 = pairs[2 * p], a2 = pairs[2 * p + 1];
+		if (a1 >= (uint32_t)N || a2 >= (uint32_t)N) return fail(ADGPU_ERR_ARG, "intramolecular pair atom out of range");
+		uint32_t t1 = ii.atom_types_const[a1], t2 = ii.atom_types_const[a2];
+		uint32_t idx = t1 * (uint32_t)nat + t2;
+		unsigned short exps = kin.VWpars_exp_const[idx];
+		uint32_t m = (exps & 0xFF00) >> 8, n = exps & 0xFF;
+		uint32_t h1 = kin.atom_types_reqm_const[t1], h2 = kin.atom_types_reqm_const[t2];
+		bool cgg0 = (h1 == 24 && h2 == 25) || (h1 == 25 && h2 == 24);   // ATYPE_CG_IDX / ATYPE_G0_IDX
+		float q1 = ii.atom_charges_const[a1], q2 = ii.atom_charges_const[a2];
+		PairRec r;
+		r.ac = kin.VWpars_AC_const[idx];
+		r.bd = kin.VWpars_BD_const[idx];
+		r.reqm = kin.reqm_AB_const[idx];
+		// same operand order as the reference's desolvation and Coulomb terms
+		r.dsolv_pref = (kin.dspars_S_const[t1] + dp.qasp * std::fabs(q1)) * kin.dspars_V_const[t2] +
+		               (kin.dspars_S_const[t2] + dp.qasp * std::fabs(q2)) * kin.dspars_V_const[t1];
+		r.qq = dp.coeff_elec * q1 * q2;
+		r.vbond = cgg0 ? 50.0f : 0.0f;
+		r.ij = a1 | (a2 << 8) | (m << 16) | (n << 24);
+		r.pad = 0;
+		pr[p] = r;
+	}
+	return ADGPU_OK;
+}
+
+adgpu_status upload_ligand(const PackedLigand& p, LigandTables& t)
+{
+	if (t.dmem && t.dmem_bytes < p.blob.size()) { cudaFree(t.dmem); t.dmem = nullptr; t.dmem_bytes = 0; }
+	if (!t.dmem) {
+		cudaError_t e = cudaMalloc(&t.dmem, p.blob.size());
+		if (e != cudaSuccess) return cuda_fail(e, "ligand tables");
+		t.dmem_bytes = p.blob.size();
+	}
+	cudaError_t e = cudaMemcpy(t.dmem, p.blob.data(), p.blob.size(), cudaMemcpyHostToDevice);
+	if (e != cudaSuccess) return cuda_fail(e, "ligand tables upload");
+	const uint8_t* D = static_cast<const uint8_t*>(t.dmem);
+	LigDev& L = t.dev;
+	L.natoms = p.natoms; L.nlig = p.nlig; L.ngenes = p.ngenes; L.ntors = p.ntors; L.npairs = p.npairs; L.ntoritems = p.ntoritems;
+	L.atom_xyzq = reinterpret_cast<const float4*>(D + p.off_atom_xyzq);
+	L.atom_info = reinterpret_cast<const uint32_t*>(D + p.off_atom_info);
+	L.chain_len = D + p.off_chain_len;
+	L.chain = D + p.off_chain;
+	L.tors_uv = reinterpret_cast<const float4*>(D + p.off_tors_uv);
+	L.tors_mv = reinterpret_cast<const float4*>(D + p.off_tors_mv);
+	L.tors_ends = reinterpret_cast<const int2*>(D + p.off_tors_ends);
+	L.tor_items = reinterpret_cast<const uint32_t*>(D + p.off_tor_items);
+	L.pairs = reinterpret_cast<const PairRec*>(D + p.off_pairs);
+	t.packed = p;
+	return ADGPU_OK;
+}
+
+void set_grid_fields(LigDev& L, const adgpu_dockpars& dp, const float* cell_grid)
+{
+	L.map_e = 0;
+	L.gx = dp.gridsize_x; L.gy = dp.gridsize_y; L.gz = dp.gridsize_z;
+	L.cells_x = dp.gridsize_x - 1;
+	L.cells_xy = (dp.gridsize_x - 1) * (dp.gridsize_y - 1);
+	L.rec_floats = 8 * (dp.num_of_map_atypes + 2);
+	L.spacing = dp.grid_spacing;
+	L.inv_spacing = 1.0f / dp.grid_spacing;
+	L.coeff_desolv = dp.coeff_desolv;
+	L.elec_min_distance = dp.elec_min_distance;
+	L.half_smooth = 0.5f * dp.smooth;
+	L.grid = cell_grid;
+}
+
+adgpu_status relayout_grid(const float* ref_grid_dev, const adgpu_dockpars& dp, float** out, size_t* out_bytes, cudaStream_t stream)
+{
+	if (dp.gridsize_x < 2 || dp.gridsize_y < 2 || dp.gridsize_z < 2 || dp.gridsize_x > 256 || dp.gridsize_y > 256 || dp.gridsize_z > 256)
+		return fail(ADGPU_ERR_LIMIT, "grid dimensions out of range 2..256");
+	size_t bytes = cell_grid_bytes(dp.gridsize_x, dp.gridsize_y, dp.gridsize_z, dp.num_of_map_atypes);
+	if (*out == nullptr || *out_bytes < bytes) {
+		if (*out) cudaFree(*out);
+		*out = nullptr;
+		cudaError_t e = cudaMalloc(out, bytes);
+		if (e != cudaSuccess) return cuda_fail(e, "cell grid");
+		*out_bytes = bytes;
+	}
+	int nmaps = dp.num_of_map_atypes + 2;
+	relayout_grid_kernel<<<148 * 8, 256, 0, stream>>>(ref_grid_dev, *out, dp.gridsize_x, dp.gridsize_y, dp.gridsize_z, nmaps, dp.num_of_map_atypes);
+	cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) return cuda_fail(e, "grid relayout launch");
+	return ADGPU_OK;
+}
+
+adgpu_status build_ligand_tables_from_device(const adgpu_gpudata& d, LigandTables& t)
+{
+	const adgpu_dockpars& dp = d.dockpars;
+	if (!d.pKerconst_interintra || !d.pKerconst_intracontrib || !d.pKerconst_intra || !d.pKerconst_rotlist ||
+	    !d.pKerconst_conform || !d.pMem_fgrids || !d.pMem_rotbonds_const || !d.pMem_rotbonds_atoms_const ||
+	    !d.pMem_num_rotating_atoms_per_rotbond_const)
+		return fail(ADGPU_ERR_ARG, "GpuData has a null table pointer");
+	if (dp.num_of_intraE_contributors < 0 || dp.num_of_intraE_contributors > ADGPU_MAX_INTRAE ||
+	    dp.rotbondlist_length < 0 || dp.rotbondlist_length > ADGPU_MAX_ROTATIONS)
+		return fail(ADGPU_ERR_LIMIT, "table sizes out of range");
+	adgpu_kc_interintra ii;
+	adgpu_kc_intra kin;
+	adgpu_kc_conform cf;
+	std::vector<uint32_t> pairs(2 * (size_t)std::max(dp.num_of_intraE_contributors, 1));
+	std::vector<int> rotlist(std::max(dp.rotbondlist_length, 1));
+	std::vector<int> rb(2 * ADGPU_MAX_ROTBONDS), rba((size_t)ADGPU_MAX_ATOMS * ADGPU_MAX_ROTBONDS), nrot(ADGPU_MAX_ROTBONDS);
+	struct { void* dst; const void* src; size_t n; } cps[] = {
+		{&ii, d.pKerconst_interintra, sizeof(ii)},
+		{&kin, d.pKerconst_intra, sizeof(kin)},
+		{&cf, d.pKerconst_conform, sizeof(cf)},
+		{pairs.data(), d.pKerconst_intracontrib, 2 * (size_t)dp.num_of_intraE_contributors * 4},
+		{rotlist.data(), d.pKerconst_rotlist, (size_t)dp.rotbondlist_length * 4},
+		{rb.data(), d.pMem_rotbonds_const, rb.size() * 4},
+		{rba.data(), d.pMem_rotbonds_atoms_const, rba.size() * 4},
+		{nrot.data(), d.pMem_num_rotating_atoms_per_rotbond_const, nrot.size() * 4},
+	};
+	for (auto& c : cps) {
+		if (c.n == 0) continue;
+		cudaError_t e = cudaMemcpy(c.dst, c.src, c.n, cudaMemcpyDeviceToHost);
+		if (e != cudaSuccess) return cuda_fail(e, "reading GpuData tables");
+	}
+	PackedLigand p;
+	adgpu_status st = pack_ligand(dp, ii, pairs.data(), kin, rotlist.data(), cf, rb.data(), rba.data(), nrot.data(), p);
+	if (st != ADGPU_OK) return st;
+	st = upload_ligand(p, t);
+	if (st != ADGPU_OK) return st;
+	t.own_grid = true;
+	st = relayout_grid(d.pMem_fgrids, dp, &t.dgrid, &t.dgrid_bytes, 0);
+	if (st != ADGPU_OK) return st;
+	cudaError_t e = cudaDeviceSynchronize();
+	if (e != cudaSuccess) return cuda_fail(e, "grid relayout");
+	set_grid_fields(t.dev, dp, t.dgrid);
+	return ADGPU_OK;
+}
+
+}  // namespace adgpu

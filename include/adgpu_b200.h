@@ -1,0 +1,258 @@
+/*
+ * adgpu_b200.h -- C ABI of the B200-native AutoDock-GPU LGA hot path.
+ *
+ * Two layers are declared here:
+ *
+ *  1. The reference's kernel API, restated as `extern "C"` entry points with
+ *     plain pointers.  A host program that today calls AutoDock-GPU's
+ *     cuda/kernels.cu API (declared in host/src/performdocking.cpp.Cuda:40-84)
+ *     can call these instead, with the same GpuData contents and the same
+ *     buffers.  libadgpu_b200 also exports the original C++-linkage names
+ *     (SetKernelsGpuData, gpu_calc_initpop, ...) so the reference host objects
+ *     link against it unchanged; those wrappers keep the reference's
+ *     print-and-exit error convention (cuda/GpuData.h:40-72), while the
+ *     adgpu_* entry points below return an adgpu_status instead.
+ *
+ *  2. A batch/serving API (adgpu_engine_*) with no reference counterpart:
+ *     many ligands with uneven atom/torsion counts, each with its own runs,
+ *     docked by one persistent launch over device-resident receptor maps.
+ *
+ * Memory ownership follows the reference: the caller allocates every buffer
+ * it passes (device pointers unless stated otherwise); the library owns only
+ * the repacked copies of the constant tables and grid that it builds inside
+ * adgpu_set_kernels_gpu_data / adgpu_engine_* calls.
+ *
+ * Layout types below must stay byte-identical to the reference's:
+ *   adgpu_dockpars            == GpuDockparameters          (cuda/GpuData.h:74-110)
+ *   adgpu_gpudata             == GpuData                    (cuda/GpuData.h:112-136)
+ *   adgpu_kc_interintra       == kernelconstant_interintra  (host/inc/calcenergy.h:88-94)
+ *   adgpu_kc_intracontrib     == kernelconstant_intracontrib(host/inc/calcenergy.h:96-99)
+ *   adgpu_kc_intra            == kernelconstant_intra       (host/inc/calcenergy.h:101-110)
+ *   adgpu_kc_rotlist          == kernelconstant_rotlist     (host/inc/calcenergy.h:112-115)
+ *   adgpu_kc_conform          == kernelconstant_conform     (host/inc/calcenergy.h:117-122)
+ *   adgpu_kc_grads            == kernelconstant_grads       (host/inc/calcenergy.h:124-136)
+ * so that a GpuData filled by the reference host program can be handed over
+ * as-is.  Limits are the reference's (common/defines.h:83-95).
+ */
+#ifndef ADGPU_B200_H
+#define ADGPU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ADGPU_MAX_ATOMS        256
+#define ADGPU_MAX_ATYPES       32
+#define ADGPU_MAX_ROTBONDS     57
+#define ADGPU_MAX_INTRAE       (ADGPU_MAX_ATOMS * ADGPU_MAX_ATOMS)
+#define ADGPU_MAX_ROTATIONS    (ADGPU_MAX_ATOMS * ADGPU_MAX_ROTBONDS)
+#define ADGPU_MAX_POPSIZE      2048
+#define ADGPU_MAX_RUNS         8192
+#define ADGPU_GENOTYPE_STRIDE  64     /* floats per genotype in global memory */
+#define ADGPU_MAX_GENES        (ADGPU_MAX_ROTBONDS + 6)
+
+typedef enum {
+	ADGPU_OK = 0,
+	ADGPU_ERR_ARG = 1,        /* bad argument (null pointer, size out of range) */
+	ADGPU_ERR_CUDA = 2,       /* a CUDA runtime call failed; see adgpu_last_error() */
+	ADGPU_ERR_NOT_READY = 3,  /* adgpu_set_kernels_gpu_data has not been called */
+	ADGPU_ERR_LIMIT = 4,      /* a reference limit (atoms, genes, runs ...) exceeded */
+	ADGPU_ERR_BUDGET = 5,     /* request does not fit the engine's memory budget */
+	ADGPU_ERR_STATE = 6,      /* call not valid in the object's current state */
+	ADGPU_ERR_TIMEOUT = 7     /* a bounded device wait gave up; kernel returned early */
+} adgpu_status;
+
+typedef struct {
+	int          num_of_atoms;
+	int          true_ligand_atoms;
+	int          num_of_atypes;
+	int          num_of_map_atypes;
+	int          num_of_intraE_contributors;
+	int          gridsize_x;
+	int          gridsize_y;
+	int          gridsize_z;
+	int          gridsize_x_times_y;
+	int          gridsize_x_times_y_times_z;
+	float        grid_spacing;
+	int          rotbondlist_length;
+	float        coeff_elec;
+	float        elec_min_distance;
+	float        coeff_desolv;
+	int          pop_size;
+	int          num_of_genes;
+	float        tournament_rate;
+	float        crossover_rate;
+	float        mutation_rate;
+	float        abs_max_dmov;
+	float        abs_max_dang;
+	float        lsearch_rate;
+	float        smooth;
+	unsigned int num_of_lsentities;
+	float        rho_lower_bound;
+	float        base_dmov_mul_sqrt3;
+	float        base_dang_mul_sqrt3;
+	unsigned int cons_limit;
+	unsigned int max_num_of_iters;
+	float        qasp;
+	float        adam_beta1;
+	float        adam_beta2;
+	float        adam_epsilon;
+} adgpu_dockpars;
+
+typedef struct {
+	float    atom_charges_const  [ADGPU_MAX_ATOMS];
+	uint32_t atom_types_const    [ADGPU_MAX_ATOMS];
+	uint32_t atom_types_map_const[ADGPU_MAX_ATOMS];
+	char     ignore_inter_const  [ADGPU_MAX_ATOMS];
+} adgpu_kc_interintra;
+
+typedef struct {
+	uint32_t intraE_contributors_const[2 * ADGPU_MAX_INTRAE];
+} adgpu_kc_intracontrib;
+
+typedef struct {
+	unsigned int   atom_types_reqm_const[ADGPU_MAX_ATYPES];
+	unsigned short VWpars_exp_const     [ADGPU_MAX_ATYPES * ADGPU_MAX_ATYPES];
+	float          reqm_AB_const        [ADGPU_MAX_ATYPES * ADGPU_MAX_ATYPES];
+	float          VWpars_AC_const      [ADGPU_MAX_ATYPES * ADGPU_MAX_ATYPES];
+	float          VWpars_BD_const      [ADGPU_MAX_ATYPES * ADGPU_MAX_ATYPES];
+	float          dspars_S_const       [ADGPU_MAX_ATYPES];
+	float          dspars_V_const       [ADGPU_MAX_ATYPES];
+} adgpu_kc_intra;
+
+typedef struct {
+	int rotlist_const[ADGPU_MAX_ROTATIONS];
+} adgpu_kc_rotlist;
+
+typedef struct {
+	float ref_coords_const             [3 * ADGPU_MAX_ATOMS];
+	float rotbonds_moving_vectors_const[3 * ADGPU_MAX_ROTBONDS];
+	float rotbonds_unit_vectors_const  [3 * ADGPU_MAX_ROTBONDS];
+} adgpu_kc_conform;
+
+typedef struct {
+	int rotbonds                      [2 * ADGPU_MAX_ROTBONDS];
+	int rotbonds_atoms                [ADGPU_MAX_ATOMS * ADGPU_MAX_ROTBONDS];
+	int num_rotating_atoms_per_rotbond[ADGPU_MAX_ROTBONDS];
+} adgpu_kc_grads;
+
+/* Rotation-list element bits (common/calcenergy_basic.h:31-36). */
+#define ADGPU_RLIST_ATOMID_MASK   0x000000FF
+#define ADGPU_RLIST_RBONDID_MASK  0x0000FF00
+#define ADGPU_RLIST_RBONDID_SHIFT 8
+#define ADGPU_RLIST_FIRSTROT_MASK 0x00010000
+#define ADGPU_RLIST_GENROT_MASK   0x00020000
+#define ADGPU_RLIST_DUMMY_MASK    0x00040000
+
+typedef struct {
+	int                     devnum;
+	int                     devid;
+	int                     preallocated_gridsize;
+	adgpu_dockpars          dockpars;
+	adgpu_kc_interintra*    pKerconst_interintra;
+	adgpu_kc_intracontrib*  pKerconst_intracontrib;
+	adgpu_kc_intra*         pKerconst_intra;
+	adgpu_kc_rotlist*       pKerconst_rotlist;
+	adgpu_kc_conform*       pKerconst_conform;
+	adgpu_kc_grads*         pKerconst_grads;
+	float*                  pMem_fgrids;
+	int*                    pMem_evals_of_new_entities;
+	int*                    pMem_gpu_evals_of_runs;
+	uint32_t*               pMem_prng_states;
+	int*                    pMem_rotbonds_const;
+	int*                    pMem_rotbonds_atoms_const;
+	int*                    pMem_num_rotating_atoms_per_rotbond_const;
+	unsigned int            warpmask;
+	unsigned int            warpbits;
+} adgpu_gpudata;
+
+/* ---------------------------------------------------------------------------
+ * Layer 1: the reference kernel API.
+ *
+ * All calls are synchronous like the reference's (its LAUNCHERROR macro
+ * synchronises after every launch, cuda/GpuData.h:49-62): results are
+ * visible to the host on return.  `threads` is accepted for signature
+ * compatibility; it names the reference's block size, which fixes how the
+ * per-thread PRNG states in pMem_prng_states are indexed (blockIdx*threads+tid,
+ * cuda/auxiliary_genetic.cu:37).  The library reproduces that indexing no
+ * matter how many device threads it actually assigns to one pose.
+ * ------------------------------------------------------------------------- */
+
+/* Replaces SetKernelsGpuData, cuda/kernels.cu:126-132.  Copies *data (device
+ * pointers inside) and builds the library's repacked tables and 8-corner grid
+ * from the pointed-to device buffers.  Must be called again whenever those
+ * buffers change. */
+adgpu_status adgpu_set_kernels_gpu_data(const adgpu_gpudata* data);
+
+/* Replaces GetKernelsGpuData, cuda/kernels.cu:134-139. */
+adgpu_status adgpu_get_kernels_gpu_data(adgpu_gpudata* data);
+
+/* Replaces gpu_calc_initpop, cuda/kernel1.cu:57-63.  blocks = runs*pop_size. */
+adgpu_status adgpu_calc_initpop(uint32_t blocks, uint32_t threads,
+                                float* conformations_current, float* energies_current);
+
+/* Replaces gpu_sum_evals, cuda/kernel2.cu:54-58.  blocks = runs. */
+adgpu_status adgpu_sum_evals(uint32_t blocks, uint32_t threads);
+
+/* Replaces gpu_gen_and_eval_newpops, cuda/kernel4.cu:307-318.  blocks = runs*pop_size. */
+adgpu_status adgpu_gen_and_eval_newpops(uint32_t blocks, uint32_t threads,
+                                        float* conformations_current, float* energies_current,
+                                        float* conformations_next, float* energies_next);
+
+/* Replaces gpu_perform_LS (Solis-Wets), cuda/kernel3.cu:311-320.  blocks = runs*num_of_lsentities. */
+adgpu_status adgpu_perform_ls(uint32_t blocks, uint32_t threads,
+                              float* conformations_next, float* energies_next);
+
+/* Replaces gpu_gradient_minAD (ADADELTA), cuda/kernel_ad.cu:396-405. */
+adgpu_status adgpu_gradient_minad(uint32_t blocks, uint32_t threads,
+                                  float* conformations_next, float* energies_next);
+
+/* Replaces gpu_gradient_minAdam (ADAM), cuda/kernel_adam.cu:399-408. */
+adgpu_status adgpu_gradient_minadam(uint32_t blocks, uint32_t threads,
+                                    float* conformations_next, float* energies_next);
+
+/* FIRE local search.  The reference has it only as an OpenCL kernel
+ * (gradient_minFire, device/kernel_fire.cl:76-895) launched from
+ * host/src/performdocking.cpp.OpenCL; same launch shape as the others. */
+adgpu_status adgpu_gradient_minfire(uint32_t blocks, uint32_t threads,
+                                    float* conformations_next, float* energies_next);
+
+/* Scores `n` genotypes (stride ADGPU_GENOTYPE_STRIDE floats, device memory)
+ * with the energy-only scorer (gpu_calc_energy, cuda/calcenergy.cu:114-453)
+ * or, if gradients != NULL, with the merged energy+gradient scorer
+ * (gpu_calc_energrad, cuda/calcMergeEneGra.cu:48-900); gradients has the same
+ * stride as genotypes.  The reference has no stand-alone entry point for its
+ * scorer; this is the unit the per-pose parity tests drive. */
+adgpu_status adgpu_score_genotypes(uint32_t n, const float* genotypes,
+                                   float* energies, float* gradients);
+
+/* Device-resident docking loop for one ligand: the generation loop of
+ * docking_with_gpu (host/src/performdocking.cpp.Cuda:684-831) without host
+ * round trips.  Runs generations (GA + the LS method `lsmet`: 0 sw, 1 ad,
+ * 2 adam, 3 fire) until the mean evaluations per run reach `max_evals` or
+ * `max_gens` generations have passed (check_progress,
+ * host/src/performdocking.cpp.Cuda:908-942), on the `num_runs` populations
+ * already resident in conformations1/energies1 (initpop and sum_evals must
+ * have run, as in the reference).  On return the final
+ * population is in the buffers reported through *final_is_second (0: 1, 1: 2)
+ * and *generations holds the number of generations executed.  Graph-captures
+ * the per-generation launch sequence. */
+adgpu_status adgpu_dock_resident(int lsmet, uint32_t num_runs, uint64_t max_evals, uint32_t max_gens,
+                                 float* conformations1, float* energies1,
+                                 float* conformations2, float* energies2,
+                                 int* final_is_second, uint32_t* generations);
+
+/* Text of the last error recorded on this thread (never NULL). */
+const char* adgpu_last_error(void);
+
+/* Library version string. */
+const char* adgpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ADGPU_B200_H */

@@ -1,0 +1,121 @@
+"""ctypes bindings of oracle/_ref/libadgpu_ref.so -- the reference's own host
+front end and CUDA kernel sources, compiled for the CPU (see oracle/Makefile).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by
+bench.py's CPU-baseline leg; never by the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libadgpu_ref.so")
+
+GENOTYPE_STRIDE = 64
+NUM_THREADS = 64      # the reference build this oracle emulates (-DN64WI)
+
+
+class RefInfo(C.Structure):
+    _fields_ = [
+        ("num_of_atoms", C.c_int), ("true_ligand_atoms", C.c_int), ("num_of_rotbonds", C.c_int),
+        ("num_of_genes", C.c_int), ("num_of_intraE_contributors", C.c_int), ("num_of_rotcyc", C.c_int),
+        ("pop_size", C.c_int), ("num_of_runs", C.c_int), ("num_of_lsentities", C.c_int),
+        ("num_of_map_atypes", C.c_int), ("gridsize", C.c_int * 3), ("spacing", C.c_float),
+        ("grid_origin", C.c_float * 3), ("nev", C.c_ulong), ("ngen", C.c_ulong), ("lsmet", C.c_char * 8),
+    ]
+
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} not built (make -C oracle ref)")
+        L = C.CDLL(LIB_PATH)
+        L.adgpu_ref_job_create.restype = C.c_void_p
+        L.adgpu_ref_job_create.argtypes = [C.c_int, C.POINTER(C.c_char_p)]
+        L.adgpu_ref_job_free.argtypes = [C.c_void_p]
+        L.adgpu_ref_job_info.argtypes = [C.c_void_p, C.POINTER(RefInfo)]
+        L.adgpu_ref_job_blob.restype = C.c_void_p
+        L.adgpu_ref_job_blob.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_size_t)]
+        L.adgpu_ref_job_bind.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.adgpu_ref_sizeof_gpudata.restype = C.c_size_t
+        L.adgpu_ref_sizeof_refgpudata.restype = C.c_size_t
+        vp = C.c_void_p
+        L.adgpu_ref_score.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp]
+        L.adgpu_ref_calc_initpop.argtypes = [C.c_uint32, C.c_uint32, vp, vp]
+        L.adgpu_ref_sum_evals.argtypes = [C.c_uint32, C.c_uint32]
+        L.adgpu_ref_gen_and_eval_newpops.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp, vp]
+        for n in ("perform_ls", "gradient_minad", "gradient_minadam"):
+            getattr(L, f"adgpu_ref_{n}").argtypes = [C.c_uint32, C.c_uint32, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class RefJob:
+    """One docking job prepared by the reference front end from a command line
+    (e.g. ['--ffile', f, '--lfile', l, '--nrun', '10', '--seed', '1,2,3'])."""
+
+    BLOB_DTYPES = {"grid": np.float32, "initpop": np.float32, "prng": np.uint32}
+
+    def __init__(self, args):
+        L = lib()
+        argv = [b"autodock_gpu"] + [a.encode() for a in args]
+        arr = (C.c_char_p * (len(argv) + 1))(*argv, None)
+        self.h = L.adgpu_ref_job_create(len(argv), arr)
+        if not self.h:
+            raise RuntimeError(f"reference setup failed for {args}")
+        self.info = RefInfo()
+        L.adgpu_ref_job_info(self.h, C.byref(self.info))
+        self._keep = []
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().adgpu_ref_job_free(self.h)
+            self.h = None
+
+    def blob(self, name: str) -> np.ndarray:
+        n = C.c_size_t()
+        p = lib().adgpu_ref_job_blob(self.h, name.encode(), C.byref(n))
+        if not p:
+            raise KeyError(name)
+        dt = self.BLOB_DTYPES.get(name, np.uint8)
+        buf = (C.c_char * n.value).from_address(p)
+        return np.frombuffer(buf, dtype=np.uint8).copy().view(dt)
+
+    def bind(self, prng: np.ndarray, evals_new: np.ndarray, evals_runs: np.ndarray, dockpars: bytes | None = None):
+        """Points the emulated kernels at this job with caller-owned state arrays."""
+        self._keep = [prng, evals_new, evals_runs]
+        dp = None
+        if dockpars is not None:
+            self._dp = C.create_string_buffer(bytes(dockpars), len(dockpars))
+            dp = C.cast(self._dp, C.c_void_p)
+        lib().adgpu_ref_job_bind(self.h, dp, _ptr(prng), _ptr(evals_new), _ptr(evals_runs))
+
+    # --- emulated reference kernels (host arrays stand in for device memory) ---
+    def score(self, genotypes: np.ndarray, gradients: bool, threads: int = NUM_THREADS):
+        g = np.ascontiguousarray(genotypes, dtype=np.float32)
+        n = g.shape[0]
+        e = np.zeros(n, np.float32)
+        gr = np.zeros((n, GENOTYPE_STRIDE), np.float32) if gradients else None
+        lib().adgpu_ref_score(n, threads, _ptr(g), _ptr(e), _ptr(gr))
+        return (e, gr) if gradients else e
+
+
+def call(name, *args):
+    L = lib()
+    conv = [(_ptr(a) if isinstance(a, np.ndarray) else a) for a in args]
+    return getattr(L, f"adgpu_ref_{name}")(*conv)

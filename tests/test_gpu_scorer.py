@@ -1,0 +1,66 @@
+"""Per-pose parity of the CUDA scorer with the oracle (energy and gene
+gradients for identical genotypes), through the C ABI."""
+import numpy as np
+import pytest
+
+import helpers
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cases(tmp_path_factory):
+    d = tmp_path_factory.mktemp("scorer")
+    return {
+        "cfg1": helpers.make_case(str(d / "cfg1"), 40, ["C", "A", "N", "OA", "HD"], 16, 4, 4, config_id=1),
+        "cfg2": helpers.make_case(str(d / "cfg2"), 60, ["C", "A", "N", "OA", "HD"], 40, 10, 4, config_id=2),
+        "flex": helpers.make_case(str(d / "flex"), 60, ["C", "A", "N", "NA", "OA", "SA", "HD"], 30, 8, 2,
+                                  config_id=4, flexres=2),
+    }
+
+
+def _activate(case):
+    from adgpu_b200 import device
+    dj = device.DeviceJob(case.tables, case.dockpars, case.grid, case.runs, case.prng)
+    dj.activate()
+    return dj
+
+
+@pytest.mark.parametrize("name", ["cfg1", "cfg2", "flex"])
+@pytest.mark.parametrize("tpp", [32, 64, 128])
+def test_energy_and_gradient_parity(cases, name, tpp, monkeypatch):
+    from adgpu_b200 import device
+    monkeypatch.setenv("ADGPU_THREADS_PER_POSE", str(tpp))
+    case = cases[name]
+    dj = _activate(case)
+    g = helpers.in_box_genotypes(case, 2000 if name != "cfg1" else 1000, seed=7)
+    e_gpu, gr_gpu = device.score(g, True)
+    e_ref, gr_ref = case.host.score(g, True, nthreads=8)
+    tol = helpers.energy_tolerance(e_ref)
+    bad = np.abs(e_gpu - e_ref) > tol
+    assert bad.sum() == 0, f"{bad.sum()} energies off, worst {np.abs(e_gpu - e_ref).max()}"
+    e_only = device.score(g, False)
+    assert np.all(np.abs(e_only - e_ref) <= tol)
+    ng = case.ngenes
+    gt = helpers.gradient_tolerance(case, gr_ref)
+    diff = np.abs(gr_gpu[:, :ng] - gr_ref[:, :ng])
+    frac_bad = (diff > gt).mean(axis=0)
+    # translation and torsion genes: every value in tolerance
+    assert frac_bad[:3].max() == 0.0
+    assert frac_bad[6:].max() <= 0.002 if ng > 6 else True
+    # orientation genes pass through an infinitesimal-rotation difference of angles
+    assert frac_bad[3:6].max() <= 0.01
+    del dj
+
+
+def test_out_of_grid_penalty(cases):
+    from adgpu_b200 import device
+    case = cases["cfg1"]
+    _activate(case)
+    g = helpers.in_box_genotypes(case, 64, seed=3)
+    g[:32, 0] = -5.0     # far outside the box
+    e_gpu, gr_gpu = device.score(g, True)
+    e_ref, gr_ref = case.host.score(g, True)
+    assert np.all(e_gpu[:32] > 1.6e7)
+    assert np.allclose(e_gpu, e_ref, rtol=1e-5)
+    assert np.allclose(gr_gpu[:32, :3], gr_ref[:32, :3])
