@@ -29,6 +29,16 @@ SIGNATURES = {
     "adgpu_gradient_minfire": (_i, [_u32, _u32, _vp, _vp]),
     "adgpu_score_genotypes": (_i, [_u32, _vp, _vp, _vp]),
     "adgpu_dock_resident": (_i, [_i, _u32, _u64, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "adgpu_grid_read": (_i, [C.c_char_p, _vp]),
+    "adgpu_grid_from_values": (_i, [_vp, C.c_double, _vp, _i, _vp, _vp, _vp]),
+    "adgpu_grid_free": (None, [_vp]),
+    "adgpu_grid_info": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "adgpu_grid_reference_layout": (_i, [_vp, _vp, C.c_size_t]),
+    "adgpu_dockpars_default": (_i, [_vp, C.c_double, _i]),
+    "adgpu_ligand_prepare": (_i, [_vp, C.c_char_p, C.c_char_p, _vp, _vp, _i, _vp]),
+    "adgpu_ligand_free": (None, [_vp]),
+    "adgpu_ligand_tables": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "adgpu_ligand_population": (_i, [_vp, _vp, C.c_size_t, _vp, C.c_size_t]),
     "adgpu_last_error": (C.c_char_p, []),
     "adgpu_version": (C.c_char_p, []),
 }

@@ -245,6 +245,57 @@ adgpu_status adgpu_dock_resident(int lsmet, uint32_t num_runs, uint64_t max_eval
                                  float* conformations2, float* energies2,
                                  int* final_is_second, uint32_t* generations);
 
+/* ---------------------------------------------------------------------------
+ * Front end: the input side of the path.  Reads AutoDock-4 grid maps and
+ * prepares PDBQT ligands (with optional flexible residues) into the
+ * reference-layout tables above, as the reference host does before it calls
+ * the kernel API.  Base AD4 atom types only (no derived types or modified
+ * pairs).  Host memory throughout.
+ * ------------------------------------------------------------------------- */
+typedef struct adgpu_grid_s adgpu_grid;
+typedef struct adgpu_ligand_s adgpu_ligand;
+
+/* Replaces get_gridinfo + get_gridvalues (host/src/processgrid.cpp:28-253):
+ * reads a .maps.fld and its .map files (type maps, then e, then d). */
+adgpu_status adgpu_grid_read(const char* fld_path, adgpu_grid** out);
+
+/* Builds a grid from values[map][z][y][x] (num_maps = type maps + e + d,
+ * types[] names the type maps followed by "e" and "d"). */
+adgpu_status adgpu_grid_from_values(const int dims[3], double spacing, const double origin[3], int num_maps,
+                                    const char* const* types, const float* values, adgpu_grid** out);
+void adgpu_grid_free(adgpu_grid* grid);
+adgpu_status adgpu_grid_info(const adgpu_grid* grid, int dims[3], double* spacing, double origin[3], int* num_map_atypes);
+
+/* The grid in the reference's device layout (4 floats per point per map,
+ * host/src/processgrid.cpp:244-248); n_floats must be 4*num_maps*X*Y*Z. */
+adgpu_status adgpu_grid_reference_layout(const adgpu_grid* grid, float* out, size_t n_floats);
+
+/* Reference defaults for every run parameter (host/inc/getparameters.h:66-145),
+ * scaled as docking_with_gpu does (host/src/performdocking.cpp.Cuda:413-463). */
+adgpu_status adgpu_dockpars_default(adgpu_dockpars* dp, double spacing, int pop_size);
+
+/* Replaces init_liganddata + parse_liganddata + gen_initpop_and_reflig +
+ * prepare_const_fields_for_gpu (host/src/processligand.cpp:40-1322,
+ * host/src/getparameters.cpp:2543-2631, host/src/calcenergy.cpp:31-488).
+ * ligand_pdbqt / flexres_pdbqt are file contents (either may be NULL, not
+ * both); run supplies the run parameters; seed is the reference's --seed
+ * triple, so the initial population and LCG states equal the reference's. */
+adgpu_status adgpu_ligand_prepare(const adgpu_grid* grid, const char* ligand_pdbqt, const char* flexres_pdbqt,
+                                  const adgpu_dockpars* run, const uint32_t seed[3], int num_runs,
+                                  adgpu_ligand** out);
+void adgpu_ligand_free(adgpu_ligand* lig);
+
+/* Copies the prepared tables out (any pointer may be NULL). */
+adgpu_status adgpu_ligand_tables(const adgpu_ligand* lig, adgpu_dockpars* dockpars,
+                                 adgpu_kc_interintra* interintra, adgpu_kc_intracontrib* intracontrib,
+                                 adgpu_kc_intra* intra, adgpu_kc_rotlist* rotlist,
+                                 adgpu_kc_conform* conform, adgpu_kc_grads* grads);
+
+/* Initial population (runs*pop_size*64 floats) and per-thread LCG states
+ * (runs*pop_size*64 uint32) of the prepared ligand. */
+adgpu_status adgpu_ligand_population(const adgpu_ligand* lig, float* initpop, size_t n_floats,
+                                     uint32_t* prng, size_t n_states);
+
 /* Text of the last error recorded on this thread (never NULL). */
 const char* adgpu_last_error(void);
 

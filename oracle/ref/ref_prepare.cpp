@@ -56,6 +56,9 @@ struct RefJob {
 	char lsmet[8] = {0};
 	float grid_origin[3] = {0, 0, 0};
 	float grid_size_angstrom[3] = {0, 0, 0};
+	std::vector<int32_t> bonds;        // [N*N] bond matrix of the prepared ligand
+	std::vector<int32_t> rigid;        // [N] rigid structure ids
+	std::vector<int32_t> contrib;      // [N*N] intramolecular contributor matrix
 };
 
 /* GpuData layout of cuda/GpuData.h:112-136, with plain pointer members. */
@@ -169,6 +172,17 @@ void* adgpu_ref_job_create(int argc, char** argv)
 	job->ngen = mypars.num_of_generations;
 	strncpy(job->lsmet, mypars.ls_method, sizeof(job->lsmet) - 1);
 	for (int i = 0; i < 3; i++) job->grid_origin[i] = (float)mygrid->origo_real_xyz[i];
+	{
+		int n = lig->num_of_atoms;
+		job->bonds.resize((size_t)n * n); job->contrib.resize((size_t)n * n); job->rigid.resize(n);
+		for (int a = 0; a < n; a++) {
+			job->rigid[a] = lig->atom_rigid_structures[a];
+			for (int b = 0; b < n; b++) {
+				job->bonds[(size_t)a * n + b] = lig->bonds[a][b];
+				job->contrib[(size_t)a * n + b] = lig->intraE_contributors[a][b];
+			}
+		}
+	}
 	delete lig; delete lig_init; delete xray;
 	return job;
 }
@@ -216,6 +230,9 @@ void* adgpu_ref_job_blob(void* h, const char* name, size_t* nbytes)
 	BLOB("grid", j->grid.data(), j->grid.size() * sizeof(float));
 	BLOB("initpop", j->initpop.data(), j->initpop.size() * sizeof(float));
 	BLOB("prng", j->prng.data(), j->prng.size() * sizeof(uint32_t));
+	BLOB("bonds", j->bonds.data(), j->bonds.size() * sizeof(int32_t));
+	BLOB("rigid", j->rigid.data(), j->rigid.size() * sizeof(int32_t));
+	BLOB("contrib", j->contrib.data(), j->contrib.size() * sizeof(int32_t));
 #undef BLOB
 	*nbytes = 0;
 	return nullptr;

@@ -69,7 +69,7 @@ class RefJob:
     """One docking job prepared by the reference front end from a command line
     (e.g. ['--ffile', f, '--lfile', l, '--nrun', '10', '--seed', '1,2,3'])."""
 
-    BLOB_DTYPES = {"grid": np.float32, "initpop": np.float32, "prng": np.uint32}
+    BLOB_DTYPES = {"grid": np.float32, "initpop": np.float32, "prng": np.uint32, "bonds": np.int32, "rigid": np.int32, "contrib": np.int32}
 
     def __init__(self, args):
         L = lib()
@@ -119,3 +119,46 @@ def call(name, *args):
     L = lib()
     conv = [(_ptr(a) if isinstance(a, np.ndarray) else a) for a in args]
     return getattr(L, f"adgpu_ref_{name}")(*conv)
+
+
+# ---------------------------------------------------------------------------
+# The reference's CUDA kernels compiled unchanged for sm_100a
+# (oracle/_ref/libadgpu_refcuda.so): same GpuData, device buffers.
+# ---------------------------------------------------------------------------
+REFCUDA_PATH = os.path.join(HERE, "_ref", "libadgpu_refcuda.so")
+_cuda = None
+
+
+def cuda_available() -> bool:
+    return os.path.exists(REFCUDA_PATH)
+
+
+def cuda_lib():
+    global _cuda
+    if _cuda is None:
+        if not cuda_available():
+            raise FileNotFoundError(f"{REFCUDA_PATH} not built (make -C oracle ref)")
+        L = C.CDLL(REFCUDA_PATH)
+        vp, u32 = C.c_void_p, C.c_uint32
+        L.adgpu_refcuda_set_gpudata.argtypes = [vp]
+        L.adgpu_refcuda_score.argtypes = [u32, vp, vp, vp]
+        L.adgpu_refcuda_score.restype = C.c_int
+        L.adgpu_refcuda_calc_initpop.argtypes = [u32, u32, vp, vp]
+        L.adgpu_refcuda_sum_evals.argtypes = [u32, u32]
+        L.adgpu_refcuda_gen_and_eval_newpops.argtypes = [u32, u32, vp, vp, vp, vp]
+        for n in ("perform_ls", "gradient_minad", "gradient_minadam"):
+            getattr(L, f"adgpu_refcuda_{n}").argtypes = [u32, u32, vp, vp]
+        _cuda = L
+    return _cuda
+
+
+def cuda_call(name, *args):
+    conv = []
+    for a in args:
+        if hasattr(a, "data_ptr"):
+            conv.append(C.c_void_p(a.data_ptr()))
+        elif isinstance(a, np.ndarray):
+            conv.append(a.ctypes.data_as(C.c_void_p))
+        else:
+            conv.append(a)
+    return getattr(cuda_lib(), f"adgpu_refcuda_{name}")(*conv)

@@ -90,6 +90,7 @@ def test_local_search(case, method, entry, oracle_fn, iters, monkeypatch):
     lib.call("adgpu_calc_initpop", R * P, T, cur, ecur)
     c_o = cur.cpu().numpy()
     e_o = ecur.cpu().numpy()
+    e_start = e_o.copy()
     prng0 = dj.prng.cpu().numpy().view(np.uint32).copy()
     st["prng"][:] = prng0
     evn0 = dj.evals_new.cpu().numpy()[:R * P].copy()
@@ -113,9 +114,9 @@ def test_local_search(case, method, entry, oracle_fn, iters, monkeypatch):
         assert added == R * L * iters
     else:
         assert R * L <= added <= R * L * iters * (2 if method == "sw" else 1)
-    # the minimisers never return a worse energy than they started with
-    if method in ("ad", "adam", "sw", "fire"):
-        assert np.all(eg[:R * P] <= e_o[:R * P] + 1e-3 * np.abs(e_o[:R * P]) + 1.0) or method != "sw"
+    # Solis-Wets only accepts improvements; the gradient methods return the best
+    # energy they evaluated, whose first evaluation is the starting genotype
+    assert np.all(eg <= e_start + 1e-4 * np.abs(e_start) + 1e-3)
 
 
 def test_resident_docking_loop(case, monkeypatch):

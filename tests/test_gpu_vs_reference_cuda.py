@@ -1,0 +1,101 @@
+"""The engine against the reference's own CUDA kernels (cuda/*.cu compiled
+unchanged for sm_100a with the reference's flags, oracle/_ref), on the same
+GPU, the same GpuData and the same PRNG states."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import helpers
+from adgpu_b200 import device, lib
+from oracle import refpy
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not refpy.cuda_available(), reason="reference CUDA kernels not built")]
+T = 64
+
+
+@pytest.fixture(scope="module")
+def case(tmp_path_factory):
+    d = tmp_path_factory.mktemp("refcuda")
+    return helpers.make_case(str(d / "cfg2"), 60, ["C", "A", "N", "OA", "HD"], 40, 10, 8, config_id=2)
+
+
+def _jobs(case, dp=None):
+    dp = dp or case.dockpars
+    dj = device.DeviceJob(case.tables, dp, case.grid, case.runs, case.prng)
+    dj.activate()
+    rj = device.DeviceJob(case.tables, dp, case.grid, case.runs, case.prng)
+    refpy.cuda_lib().adgpu_refcuda_set_gpudata(C.cast(C.pointer(rj.g), C.c_void_p))
+    return dj, rj
+
+
+def test_scorer_matches_reference_cuda(case):
+    dj, rj = _jobs(case)
+    g = helpers.in_box_genotypes(case, 4000, seed=21)
+    e_me, gr_me = device.score(g, True)
+    gt = torch.from_numpy(g).cuda()
+    e_ref = torch.zeros(len(g), device="cuda")
+    gr_ref = torch.zeros_like(gt)
+    assert refpy.cuda_call("score", len(g), gt, e_ref, gr_ref) == 0
+    e_ref, gr_ref = e_ref.cpu().numpy(), gr_ref.cpu().numpy()
+    # the reference runs with -use_fast_math (__sinf, __powf, approximate division)
+    assert np.all(np.abs(e_me - e_ref) <= 1e-4 * np.abs(e_ref) + 1e-3)
+    ng = case.ngenes
+    bad = np.abs(gr_me[:, :ng] - gr_ref[:, :ng]) > helpers.gradient_tolerance(case, gr_ref)
+    assert bad[:, :3].mean() <= 0.002 and bad[:, 6:].mean() <= 0.01 and bad[:, 3:6].mean() <= 0.02
+
+
+def test_ga_generation_matches_reference_cuda(case):
+    dj, rj = _jobs(case)
+    R, P = case.runs, case.dockpars.pop_size
+    cur, ecur = dj.population(case.initpop)
+    lib.call("adgpu_calc_initpop", R * P, T, cur, ecur)
+    n1, e1 = dj.population()
+    n2, e2 = rj.population()
+    lib.call("adgpu_gen_and_eval_newpops", R * P, T, cur, ecur, n1, e1)
+    refpy.cuda_call("gen_and_eval_newpops", R * P, T, cur, ecur, n2, e2)
+    torch.cuda.synchronize()
+    assert torch.equal(dj.prng, rj.prng)
+    ng = case.ngenes
+    assert torch.equal(n1[:, :ng], n2[:, :ng])
+    a, b = e1.cpu().numpy(), e2.cpu().numpy()
+    assert np.all(np.abs(a - b) <= 1e-4 * np.abs(b) + 1e-3)
+
+
+def test_solis_wets_draw_order_matches_reference_cuda(case):
+    dp = case.dockpars.copy()
+    dp.max_num_of_iters = 1
+    dj, rj = _jobs(case, dp)
+    R, P, L = case.runs, dp.pop_size, dp.num_of_lsentities
+    cur, ecur = dj.population(case.initpop)
+    lib.call("adgpu_calc_initpop", R * P, T, cur, ecur)
+    c2, e2 = cur.clone(), ecur.clone()
+    lib.call("adgpu_perform_ls", R * L, T, cur, ecur)
+    refpy.cuda_call("perform_ls", R * L, T, c2, e2)
+    torch.cuda.synchronize()
+    # identical LCG consumption, identical deviates
+    assert torch.equal(dj.prng, rj.prng)
+    ng = case.ngenes
+    same = (torch.abs(cur[:, :ng] - c2[:, :ng]).amax(dim=1) <= 1e-3).float().mean().item()
+    assert same >= 0.98
+
+
+@pytest.mark.parametrize("entry,name", [("adgpu_gradient_minad", "gradient_minad"),
+                                        ("adgpu_gradient_minadam", "gradient_minadam")])
+def test_gradient_ls_matches_reference_cuda_short(case, entry, name):
+    dp = case.dockpars.copy()
+    dp.max_num_of_iters = 3
+    dj, rj = _jobs(case, dp)
+    R, P, L = case.runs, dp.pop_size, dp.num_of_lsentities
+    cur, ecur = dj.population(case.initpop)
+    lib.call("adgpu_calc_initpop", R * P, T, cur, ecur)
+    c2, e2 = cur.clone(), ecur.clone()
+    lib.call(entry, R * L, T, cur, ecur)
+    refpy.cuda_call(name, R * L, T, c2, e2)
+    torch.cuda.synchronize()
+    assert torch.equal(dj.prng, rj.prng)
+    ng = case.ngenes
+    same = (torch.abs(cur[:, :ng] - c2[:, :ng]).amax(dim=1) <= 1e-1).float().mean().item()
+    assert same >= 0.95
