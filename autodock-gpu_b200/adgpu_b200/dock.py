@@ -1,0 +1,49 @@
+"""Plain per-ligand docking through the reference kernel API: the call
+sequence of docking_with_gpu (host/src/performdocking.cpp.Cuda:640-831) --
+initial population, eval sums, then the generation loop -- with the loop
+resident on the device (adgpu_dock_resident)."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import abi, lib
+from .device import DeviceJob
+
+LSMET = {"sw": 0, "ad": 1, "adam": 2, "fire": 3}
+REF_THREADS = 64
+
+
+@dataclass
+class DockResult:
+    conformations: torch.Tensor     # final population [runs*pop, 64]
+    energies: torch.Tensor          # [runs*pop]
+    evals_per_run: np.ndarray       # [runs]
+    generations: int
+
+
+def dock(job: DeviceJob, initpop: np.ndarray | torch.Tensor, lsmet: str = "ad", nev: int = 2_500_000,
+         ngen: int = 42_000, buffers=None) -> DockResult:
+    """Docks the active ligand: runs*pop entities from `initpop`, until the
+    mean evaluations per run reach `nev` or `ngen` generations have run."""
+    R, P = job.runs, job.dp.pop_size
+    if buffers is None:
+        c1, e1 = job.population()
+        c2, e2 = job.population()
+    else:
+        c1, e1, c2, e2 = buffers
+    if isinstance(initpop, torch.Tensor):
+        c1.copy_(initpop[:R * P])
+    else:
+        c1.copy_(torch.from_numpy(np.ascontiguousarray(initpop[:R * P], np.float32)))
+    job.evals_runs.zero_()
+    lib.call("adgpu_calc_initpop", R * P, REF_THREADS, c1, e1)
+    lib.call("adgpu_sum_evals", R, REF_THREADS)
+    fin = C.c_int(0)
+    gens = C.c_uint32(0)
+    lib.call("adgpu_dock_resident", LSMET[lsmet], R, int(nev), int(ngen), c1, e1, c2, e2, C.byref(fin), C.byref(gens))
+    c, e = (c2, e2) if fin.value else (c1, e1)
+    return DockResult(c, e, job.evals_runs.cpu().numpy().copy(), gens.value)

@@ -11,6 +11,10 @@
 #include "adgpu_kernels.cuh"
 #include "adgpu_tables.h"
 
+#ifndef ADGPU_MIN_CTAS
+#define ADGPU_MIN_CTAS 6     // 6 CTAs x 4 warps per SM: <= 80 registers, no spills
+#endif
+
 namespace adgpu {
 
 thread_local std::string g_last_error;
@@ -33,14 +37,30 @@ adgpu_status cuda_fail(cudaError_t e, const char* what)
 // kernels
 // ---------------------------------------------------------------------------
 template <int TPP, int KIND>
-__global__ void __launch_bounds__(256) lga_kernel(KArgs a, float* grads)
+__global__ void __launch_bounds__(128, ADGPU_MIN_CTAS) lga_kernel(KArgs a, float* grads)
 {
 	if (a.stop_flag && *a.stop_flag) return;
 	int gid, ngroups;
 	Group<TPP> G;
 	GroupSmem S;
 	group_of<TPP>(a, gid, ngroups, G, S);
-	for (uint32_t b = gid; b < a.nblocks; b += ngroups) {
+	// Local searches run for a data-dependent number of iterations, so pose
+	// groups take the next block from a counter instead of a fixed stride.
+	auto next = [&](uint32_t cur) -> uint32_t {
+		if (a.work_counter == nullptr) return cur + ngroups;
+		uint32_t b = 0;
+		if (G.rank == 0) b = atomicAdd(a.work_counter, 1u) + (uint32_t)ngroups;
+		if constexpr (TPP == 32) {
+			b = __shfl_sync(0xffffffffu, b, 0);
+		} else {
+			if (G.rank == 0) S.misc[15] = (int)b;
+			G.sync();
+			b = (uint32_t)S.misc[15];
+			G.sync();
+		}
+		return b;
+	};
+	for (uint32_t b = gid; b < a.nblocks; b = next(b)) {
 		if constexpr (KIND == 0) ga_block<TPP>(a, b, G, S);
 		else if constexpr (KIND == 1) sw_block<TPP>(a, b, G, S);
 		else if constexpr (KIND == 2) gradient_ls_block<TPP, LS_AD>(a, b, G, S);
@@ -161,6 +181,7 @@ struct ApiState {
 	adgpu_gpudata data;
 	LigandTables tables;       // host-repacked + device copy
 	int tpp = 32;
+	unsigned int* counters = nullptr;   // library-owned work counters of the local-search launches
 	std::mutex mu;
 };
 
@@ -236,6 +257,8 @@ adgpu_status dock_resident(ApiState& s, int lsmet, uint32_t runs, uint64_t max_e
 			KArgs l = a;
 			l.nblocks = runs * dp.num_of_lsentities;
 			l.conf = cn; l.e = en;
+			l.work_counter = s.counters + 1 + half;
+			cudaMemsetAsync(l.work_counter, 0, sizeof(unsigned int), st);
 			switch (ls_kind) {
 			case 1: rc = launch_kind<1>(l, nullptr, st, s.tpp); break;
 			case 2: rc = launch_kind<2>(l, nullptr, st, s.tpp); break;
@@ -284,6 +307,7 @@ adgpu_status adgpu_set_kernels_gpu_data(const adgpu_gpudata* data)
 	adgpu_status st = build_ligand_tables_from_device(*data, s.tables);
 	if (st != ADGPU_OK) return st;
 	if (const char* t = getenv("ADGPU_THREADS_PER_POSE")) s.tpp = atoi(t);
+	if (!s.counters) ADGPU_CUDA(cudaMalloc(&s.counters, 16 * sizeof(unsigned int)), "work counters");
 	s.ready = true;
 	return ADGPU_OK;
 }
@@ -308,6 +332,10 @@ static adgpu_status run_kind(int kind, uint32_t blocks, uint32_t threads, const 
 	a.ref_threads = threads;
 	a.nblocks = blocks;
 	a.conf_cur = cc; a.e_cur = ec; a.conf = conf; a.e = e;
+	if (kind >= 1 && kind <= 4) {
+		ADGPU_CUDA(cudaMemsetAsync(s.counters, 0, sizeof(unsigned int), 0), "work counter reset");
+		a.work_counter = s.counters;
+	}
 	switch (kind) {
 	case 0: st = launch_kind<0>(a, grads, 0, s.tpp); break;
 	case 1: st = launch_kind<1>(a, grads, 0, s.tpp); break;

@@ -334,47 +334,58 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	if (GRAD) G.sync();
 
 	// 4. intramolecular pairs (cuda/calcMergeEneGra.cu:418-602)
+	// The reference's terms, rewritten with one reciprocal square root and two
+	// reciprocals per pair instead of divisions and __powf:
+	//   (AC - sd^(m-n) BD) sd^-m = AC/sd^m - BD/sd^n  (m = 12, n = 6 or 10)
 	for (int p = rank; p < L.npairs; p += TPP) {
 		const float4* pr = reinterpret_cast<const float4*>(L.pairs + p);
 		float4 A = __ldg(pr), B = __ldg(pr + 1);
 		uint32_t ij = __float_as_uint(B.z);
-		int a1 = ij & 0xFF, a2 = (ij >> 8) & 0xFF, m = (ij >> 16) & 0xFF, n = ij >> 24;
+		int a1 = ij & 0xFF, a2 = (ij >> 8) & 0xFF;
 		float subx = S.x[a1] - S.x[a2], suby = S.y[a1] - S.y[a2], subz = S.z[a1] - S.z[a2];
-		float dist = sqrtf(subx * subx + suby * suby + subz * subz);
+		float d2g = subx * subx + suby * suby + subz * subz;
+		float inv_dist = rsqrtf(d2g);
+		float dist = d2g > 0.0f ? d2g * inv_dist : 0.0f;
 		float r = dist * L.spacing;
 		float pg = B.y;                       // vbond (G for CG-G0 pairs)
 		e_acc += B.y * r;
 		if (r < 8.0f) {
-			float delta = A.z - r, sd;
-			if (fabsf(delta) >= L.half_smooth) sd = r + copysignf(L.half_smooth, delta);
-			else sd = A.z;
-			// integer powers by repeated multiplication: s^(m-n) and s^-m
-			float inv = 1.0f / sd;
-			float rm = 1.0f, rmn = 1.0f;
-			{
+			float delta = A.z - r;
+			float sd = (fabsf(delta) >= L.half_smooth) ? r + copysignf(L.half_smooth, delta) : A.z;
+			float inv = __fdividef(1.0f, sd);
+			float i2 = inv * inv, i4 = i2 * i2, i6 = i4 * i2, i12 = i6 * i6;
+			uint32_t mn = ij >> 16;           // m | n << 8
+			float im, in_, fm, fn;
+			if (mn == (12u | (6u << 8))) { im = i12; in_ = i6; fm = 12.0f; fn = 6.0f; }
+			else if (mn == (12u | (10u << 8))) { im = i12; in_ = i6 * i4; fm = 12.0f; fn = 10.0f; }
+			else {
+				// general exponents (modified pair potentials): inv^m, inv^n by squaring
+				int m = mn & 0xFF, n = mn >> 8;
+				im = 1.0f; in_ = 1.0f;
 				float b = inv; int e = m;
-				while (e) { if (e & 1) rm *= b; b *= b; e >>= 1; }
-				int k = m - n;
-				if (k >= 0) { b = sd; e = k; } else { b = inv; e = -k; }
-				while (e) { if (e & 1) rmn *= b; b *= b; e >>= 1; }
+				while (e) { if (e & 1) im *= b; b *= b; e >>= 1; }
+				b = inv; e = n;
+				while (e) { if (e & 1) in_ *= b; b *= b; e >>= 1; }
+				fm = (float)m; fn = (float)n;
 			}
-			e_acc += (A.x - rmn * A.y) * rm;
-			if (GRAD) pg += ((float)n * A.y * rmn - (float)m * A.x) * rm * inv;
+			e_acc += A.x * im - A.y * in_;
+			if (GRAD) pg += (fn * A.y * in_ - fm * A.x * im) * inv;
 		}
 		if (r < 20.48f) {
-			if (r < L.elec_min_distance) r = L.elec_min_distance;
+			float inv_r = inv_dist * L.inv_spacing;
+			if (r < L.elec_min_distance) { r = L.elec_min_distance; inv_r = __fdividef(1.0f, r); }
 			float d2 = r * r;
-			float desolv = A.w * (L.coeff_desolv * (12.96f - 0.1063f * d2 * (1.0f - 0.001947f * d2)) /
-			                      (12.96f + d2 * (0.4137f + d2 * (0.00357f + 0.000112f * d2))));
-			float shift = r + 1.26366f;
-			float s2 = shift * shift;
-			float diel = 1.10859f / s2 + 0.010358f;
-			float es = B.x / r;
+			float desolv = A.w * __fdividef(L.coeff_desolv * (12.96f - 0.1063f * d2 * (1.0f - 0.001947f * d2)),
+			                                (12.96f + d2 * (0.4137f + d2 * (0.00357f + 0.000112f * d2))));
+			float rs = __fdividef(1.0f, r + 1.26366f);
+			float rs2 = rs * rs;
+			float diel = 1.10859f * rs2 + 0.010358f;
+			float es = B.x * inv_r;
 			e_acc += diel * es + desolv;
-			if (GRAD) pg += -(es / r) * diel - es * 2.21718f / (s2 * shift) - 0.0771605f * r * desolv;
+			if (GRAD) pg += -(es * inv_r) * diel - es * 2.21718f * rs2 * rs - 0.0771605f * r * desolv;
 		}
 		if (GRAD) {
-			float gdd = -pg / dist;
+			float gdd = -pg * inv_dist;
 			int ix = quant(subx * gdd), iy = quant(suby * gdd), iz = quant(subz * gdd);
 			atomicSub(&S.fx[a1], ix); atomicSub(&S.fy[a1], iy); atomicSub(&S.fz[a1], iz);
 			atomicAdd(&S.fx[a2], ix); atomicAdd(&S.fy[a2], iy); atomicAdd(&S.fz[a2], iz);

@@ -30,6 +30,7 @@ struct KArgs {
 	uint32_t nblocks;           // reference blocks (entities) in this launch
 	uint32_t ref_threads;       // reference block size (PRNG layout)
 	const int* stop_flag;       // nullable: when *stop_flag != 0 the launch does nothing
+	unsigned int* work_counter; // nullable: zeroed before the launch; pose groups take blocks from it
 };
 
 // Per-group scratch carved from dynamic shared memory.

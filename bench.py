@@ -1,0 +1,426 @@
+"""Benchmark of the LGA docking hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--lsmet ad|sw|adam|fire]
+
+Workload (the plain per-ligand configuration): one synthetic receptor
+(60^3 grid points at 0.375 A; C, A, N, OA, HD, e and d maps) and one seeded
+ligand of 40 heavy atoms with 10 torsions, nrun 100, population 150,
+2.5M evaluations per run.  One step = one complete docking of that ligand
+(initial population, then generations of GA + local search until the mean
+evaluations per run reach 2.5M), through the reference kernel API
+(libadgpu_b200).  The metric is score evaluations per second, counted the
+way the reference counts them (per-run eval counters), plus ligands/hour.
+
+With N > 1 (torchrun), every rank docks its own ligand on its own GPU: the
+ligands are independent, there is no data-path collective (replicas), and
+`value` is all ranks' evaluations over the slowest rank's time.
+
+--impl reference times the reference's algorithm on the host cores: the C
+restatement of the reference kernels (oracle/, one pose per thread, all
+host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "autodock-gpu_b200")]
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = dict(npts=60, types=["C", "A", "N", "OA", "HD"], n_heavy=40, n_tors=10, nrun=100, pop=150,
+                nev=2_500_000, config_id=2, seed=(305419896, 2271560481, 3735928559))
+METRIC = "score-evals/s"
+UNIT = "evals/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def build_inputs(lsmet: str, rank: int = 0):
+    """Seeded synthetic receptor + ligand, prepared by the engine's front end."""
+    from adgpu_b200 import frontend, synth
+    w = WORKLOAD
+    spec = synth.grid_spec(w["npts"], w["types"], seed=12345 + w["config_id"])
+    maps = synth.quantize_maps(synth.make_maps(spec))
+    grid = frontend.Grid.from_maps(maps, w["types"], spec.spacing, spec.origin)
+    mol = synth.ligand_for(w["config_id"], rank, w["n_heavy"], w["n_tors"])
+    lines, _ = synth.pdbqt_lines(mol)
+    text = "\n".join(lines) + "\n"
+    run = frontend.default_dockpars(grid.spacing, w["pop"])
+    lig = frontend.Ligand(grid, text, None, run=run, seed=w["seed"], num_runs=w["nrun"])
+    return grid, lig
+
+
+def cost_model(lig):
+    """Algorithmic FLOPs per evaluation from the prepared tables:
+    40*R_rot + 200*N_i + 80*Q + 25*S_tors + 30*N (energy+gradient) and
+    40*R_rot + 100*N_i + 45*Q (energy only); bytes = 96*N_i (3 maps x 8 corners x 4 B)."""
+    from adgpu_b200 import abi
+    dp = lig.dockpars
+    N, Q = dp.num_of_atoms, dp.num_of_intraE_contributors
+    ii = np.frombuffer(bytes(lig.tables["interintra"]), np.uint8)
+    n_i = int((ii[3072:3072 + N] == 0).sum())
+    rl = np.frombuffer(bytes(lig.tables["rotlist"]), np.int32)[:dp.rotbondlist_length]
+    r_rot = int(((rl & abi.RLIST_DUMMY_MASK) == 0).sum())
+    gr = abi.KcGrads.from_buffer_copy(bytes(lig.tables["grads"]))
+    s_tors = int(sum(gr.num_rotating_atoms_per_rotbond[:dp.num_of_genes - 6]))
+    grad = 40 * r_rot + 200 * n_i + 80 * Q + 25 * s_tors + 30 * N
+    energy = 40 * r_rot + 100 * n_i + 45 * Q
+    return dict(N=N, N_i=n_i, Q=Q, R_rot=r_rot, S_tors=s_tors, flop_grad=grad, flop_energy=energy, bytes=96 * n_i)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                smax = float(p[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        load = [s for s in sm if smax and s > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(lig, lsmet: str, budget_s: float = 15.0):
+    """The oracle (C restatement of the reference kernels, one pose per host
+    thread) on a bounded sample: local searches of the initial population."""
+    from oracle import oraclepy
+    from adgpu_b200 import abi
+    nthreads = os.cpu_count() or 1
+    ht = oraclepy.HostTables(lig.tables, lig.dockpars, _reference_grid_cache["grid"])
+    P = lig.dockpars.pop_size
+    runs = 2
+    pop = lig.initpop[:runs * P].copy()
+    en = np.zeros(runs * P, np.int32)
+    er = np.zeros(runs, np.int32)
+    ht.bind_state(lig.prng.copy(), en, er)
+    e = ht.score(pop, False, nthreads=nthreads)
+    fn = {"ad": "gradient_minad", "sw": "perform_ls", "adam": "gradient_minadam", "fire": "gradient_minfire"}[lsmet]
+    L = lig.dockpars.num_of_lsentities
+    evals, t0 = 0, time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t0 < budget_s:
+        c = pop.copy()
+        ee = e.copy()
+        en[:] = 0
+        ht.call(fn, runs * L, 64, c, ee, nthreads)
+        evals += int(en.sum())
+        reps += 1
+    dt = time.perf_counter() - t0
+    return {"value": evals / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{reps} x {lsmet} local search of {runs}x{L} entities of the workload's initial population "
+                      f"({evals} evals, {dt:.1f} s) on {nthreads} host threads"}
+
+
+_reference_grid_cache = {}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference algorithm on the host cores."""
+    if rank != 0:
+        return None
+    grid, lig = build_inputs(args.lsmet)
+    _reference_grid_cache["grid"] = grid.reference_layout()
+    steps = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(lig, args.lsmet, budget_s=max(3.0, 20.0 / max(1, args.steps + args.warmup)))
+        if i >= args.warmup:
+            steps.append(cb)
+    v = sum(s["value"] for s in steps) / len(steps)
+    w = WORKLOAD
+    evals_per_docking = w["nrun"] * w["nev"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * evals_per_docking / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": _config(args), "ligands_per_hour": 3600.0 * v / evals_per_docking,
+            "cpu_baseline": steps[-1] | {"value": v},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def _config(args):
+    w = WORKLOAD
+    return {"workload": f"plain per-ligand docking: {w['npts']}^3 maps (5 types + e + d), ligand {w['n_heavy']} heavy "
+                        f"atoms / {w['n_tors']} torsions, nrun {w['nrun']}, pop {w['pop']}, nev {w['nev']}, "
+                        f"lsmet {args.lsmet}",
+            "lsmet": args.lsmet, "nrun": w["nrun"], "pop_size": w["pop"], "nev_per_run": w["nev"],
+            "grid_points": w["npts"] + 1, "l2": "flushed between timed steps (256 MiB write)",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def run_engine(args, rank, world, local_rank):
+    import torch
+    from adgpu_b200 import device, dock, lib
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    grid, lig = build_inputs(args.lsmet, rank)
+    ref_grid = grid.reference_layout()
+    _reference_grid_cache["grid"] = ref_grid
+    w = WORKLOAD
+    job = device.DeviceJob(lig.tables, lig.dockpars, ref_grid, w["nrun"], lig.prng, device=dev)
+    job.activate()
+    bufs = (*job.population(), *job.population())
+    init_dev = torch.from_numpy(lig.initpop).to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    prng0 = job.prng.clone()
+
+    def one_docking():
+        job.prng.copy_(prng0)
+        return dock.dock(job, init_dev, args.lsmet, w["nev"], 42000, buffers=bufs)
+
+    for _ in range(args.warmup):
+        one_docking()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    times, evals, gens = [], 0, 0
+    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev_a.record()
+        res = one_docking()
+        ev_b.record()
+        torch.cuda.synchronize()
+        times.append(ev_a.elapsed_time(ev_b) / 1e3)
+        evals += int(res.evals_per_run.sum())
+        gens += res.generations
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    t_local = sum(times)
+    t_all = t_local
+    ev_all = evals
+    if world > 1:
+        t = torch.tensor([t_local], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e = torch.tensor([float(evals)], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(e, op=torch.distributed.ReduceOp.SUM)
+        t_all, ev_all = float(t.item()), int(e.item())
+    value = ev_all / t_all
+    best = float(res.energies.min().item())
+
+    # --- end to end through the public API with host buffers -------------------
+    host_grid = ref_grid
+    host_tables = lig.tables
+    host_pop = np.ascontiguousarray(lig.initpop, np.float32)
+    host_prng = lig.prng
+    e2e_times, e2e_evals = [], 0
+    h2d = host_grid.nbytes + sum(np.asarray(t).nbytes for t in host_tables.values()) + host_pop.nbytes + host_prng.nbytes
+    d2h = 0
+    for i in range(max(1, min(args.steps, 2))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        j2 = device.DeviceJob(host_tables, lig.dockpars, host_grid, w["nrun"], host_prng, device=dev)
+        j2.activate()
+        pop_dev = torch.from_numpy(host_pop).to(dev)
+        r2 = dock.dock(j2, pop_dev, args.lsmet, w["nev"], 42000)
+        conf_h = r2.conformations.cpu().numpy()
+        en_h = r2.energies.cpu().numpy()
+        e2e_times.append(time.perf_counter() - t0)
+        e2e_evals += int(r2.evals_per_run.sum())
+        d2h = conf_h.nbytes + en_h.nbytes + r2.evals_per_run.nbytes
+        del j2
+    job.activate()
+    e2e_local = sum(e2e_times)
+    e2e_value = e2e_evals / e2e_local
+    if world > 1:
+        t = torch.tensor([e2e_local], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e = torch.tensor([float(e2e_evals)], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(e, op=torch.distributed.ReduceOp.SUM)
+        e2e_value = float(e.item()) / float(t.item())
+
+    # --- roofline of the dominant kernel (the local search) -------------------------
+    cm = cost_model(lig)
+    roof = None
+    if rank == 0:
+        mid = dock.dock(job, init_dev, args.lsmet, w["nev"], 10, buffers=bufs)   # a mid-docking population
+        c_mid, e_mid = mid.conformations.clone(), mid.energies.clone()
+        entry = {"ad": "adgpu_gradient_minad", "sw": "adgpu_perform_ls", "adam": "adgpu_gradient_minadam",
+                 "fire": "adgpu_gradient_minfire"}[args.lsmet]
+        L = lig.dockpars.num_of_lsentities
+        durs, ls_evals = [], []
+        for _ in range(3):
+            c, e = c_mid.clone(), e_mid.clone()
+            job.evals_new.zero_()
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev_a.record()
+            lib.call(entry, w["nrun"] * L, 64, c, e)
+            ev_b.record()
+            torch.cuda.synchronize()
+            durs.append(ev_a.elapsed_time(ev_b) / 1e3)
+            ls_evals.append(int(job.evals_new.sum().item()))
+        dur = statistics.mean(durs)
+        flop_per_eval = cm["flop_grad"] if args.lsmet != "sw" else cm["flop_energy"]
+        achieved = statistics.mean(ls_evals) * flop_per_eval / dur / 1e12
+        scratch = torch.empty(4096 * 1024, dtype=torch.float32, device=dev)
+        import ctypes as C
+        peak = C.c_float(0)
+        lib.call("adgpu_measure_fp32_peak", scratch, scratch.numel(), C.byref(peak))
+        traffic = None
+        tfile = os.path.join(ROOT, "profiles", "ls_kernel_traffic.json")
+        if os.path.exists(tfile):
+            try:
+                traffic = json.load(open(tfile)).get(args.lsmet)
+            except Exception:
+                traffic = None
+        roof = {"bound": "fp32", "achieved": achieved, "peak": float(peak.value), "unit": "TFLOP/s",
+                "frac": achieved / float(peak.value), "traffic": traffic,
+                "peak_source": "measured in this run (FMA-chain probe, adgpu_measure_fp32_peak); "
+                               "MEASURED_PEAKS.json has no FP32 figure",
+                "kernel": entry, "launch_ms": dur * 1e3, "evals_per_launch": statistics.mean(ls_evals),
+                "flop_per_eval": flop_per_eval, "bytes_per_eval": cm["bytes"],
+                "hbm_frac_of_measured": (statistics.mean(ls_evals) * cm["bytes"] / dur / 1e9) / _hbm_peak()}
+
+    line = None
+    if rank == 0:
+        evals_per_docking = w["nrun"] * w["nev"]
+        gl = gens // max(1, args.steps)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+                "config": _config(args) | {"n_gpus": world},
+                "ligands_per_hour": 3600.0 * world * args.steps / t_all,
+                "generations_per_docking": gl, "best_energy": best,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                # per docking: initpop + sum_evals + graphs of 2 generations x 4 kernels, polled every 4 graphs
+                "gpu_launches": int(args.steps * (2 + 32 * -(-(gl + 1) // 8))),
+                "clocks": clocks, "roofline": roof, "cost_model": cm}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(lig, args.lsmet)
+        del evals_per_docking
+    return line
+
+
+def run_kernel_only(args):
+    """--mode ls-kernel: one docking cut after a few generations, then `--steps`
+    launches of the local-search kernel alone on that population (the case
+    the ncu captures use; --nrun keeps it small)."""
+    import torch
+    from adgpu_b200 import device, dock, lib
+    grid, lig = build_inputs(args.lsmet)
+    ref_grid = grid.reference_layout()
+    w = WORKLOAD
+    nrun = args.nrun or w["nrun"]
+    job = device.DeviceJob(lig.tables, lig.dockpars, ref_grid, nrun, lig.prng)
+    # the docking that produces the population runs with 64 threads per pose
+    # so that a profiler can select the measured 32-thread launches by name
+    os.environ["ADGPU_THREADS_PER_POSE"] = "64"
+    job.activate()
+    init_dev = torch.from_numpy(lig.initpop[:nrun * w["pop"]]).cuda()
+    mid = dock.dock(job, init_dev, args.lsmet, w["nev"], 10)
+    os.environ["ADGPU_THREADS_PER_POSE"] = str(args.tpp)
+    job.activate()
+    entry = {"ad": "adgpu_gradient_minad", "sw": "adgpu_perform_ls", "adam": "adgpu_gradient_minadam",
+             "fire": "adgpu_gradient_minfire"}[args.lsmet]
+    L = lig.dockpars.num_of_lsentities
+    for _ in range(args.steps):
+        c, e = mid.conformations.clone(), mid.energies.clone()
+        job.evals_new.zero_()
+        lib.call(entry, nrun * L, 64, c, e)
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "ls-kernel", "kernel": entry, "nrun": nrun, "launches": args.steps,
+                      "evals_last_launch": int(job.evals_new.sum().item())}))
+
+
+def _hbm_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--lsmet", default="ad", choices=["ad", "sw", "adam", "fire"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel"])
+    ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel mode)")
+    ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
+    args = ap.parse_args()
+    if args.mode == "ls-kernel":
+        run_kernel_only(args)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line = run_engine(args, rank, world, local_rank)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -296,6 +296,11 @@ adgpu_status adgpu_ligand_tables(const adgpu_ligand* lig, adgpu_dockpars* dockpa
 adgpu_status adgpu_ligand_population(const adgpu_ligand* lig, float* initpop, size_t n_floats,
                                      uint32_t* prng, size_t n_states);
 
+/* Measurement helper (no counterpart in the reference): measured FP32 FMA
+ * throughput of the current device in TFLOP/s, the denominator of the
+ * scorer's roofline fraction.  device_scratch must hold 2048 floats per SM. */
+adgpu_status adgpu_measure_fp32_peak(float* device_scratch, size_t n_floats, float* tflops);
+
 /* Text of the last error recorded on this thread (never NULL). */
 const char* adgpu_last_error(void);
 

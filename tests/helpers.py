@@ -104,3 +104,19 @@ def gradient_tolerance(case: Case, ref: np.ndarray) -> np.ndarray:
     floor[6:] = quantum[6:] * 16.0
     del n_terms
     return 1e-4 * np.abs(ref[..., :ng]) + floor
+
+
+def gradient_bound(case: Case, ref: np.ndarray) -> np.ndarray:
+    """Worst-case per-gene bound: 1e-4 relative plus one quantum (1/1024, in
+    gene units) per quantised term that feeds the gene (every atom's inter
+    term and both ends of every intramolecular pair); the orientation genes get
+    the same bound amplified by the 1/INFINITESIMAL_RADIAN (1e3) step through
+    which torques become angle differences (cuda/calcMergeEneGra.cu:701-815)."""
+    ng = case.ngenes
+    n_terms = case.info.num_of_atoms + 2 * case.info.num_of_intraE_contributors
+    sp = case.info.spacing
+    scale = np.ones(ng, np.float64)
+    scale[3:] = sp * sp / (0.0174533 ** 2)
+    bound = scale * n_terms / 1024.0
+    bound[3:6] *= 1e3 / 1024.0 * 8.0
+    return 1e-4 * np.abs(ref[..., :ng]) + bound

@@ -42,14 +42,16 @@ def test_energy_and_gradient_parity(cases, name, tpp, monkeypatch):
     e_only = device.score(g, False)
     assert np.all(np.abs(e_only - e_ref) <= tol)
     ng = case.ngenes
-    gt = helpers.gradient_tolerance(case, gr_ref)
     diff = np.abs(gr_gpu[:, :ng] - gr_ref[:, :ng])
-    frac_bad = (diff > gt).mean(axis=0)
-    # translation and torsion genes: every value in tolerance
-    assert frac_bad[:3].max() == 0.0
+    # tier 1 (typical pose): 1e-4 relative plus a few fixed-point quanta
+    frac_bad = (diff > helpers.gradient_tolerance(case, gr_ref)).mean(axis=0)
+    assert frac_bad[:3].max() <= 0.002
     assert frac_bad[6:].max() <= 0.002 if ng > 6 else True
     # orientation genes pass through an infinitesimal-rotation difference of angles
     assert frac_bad[3:6].max() <= 0.01
+    # tier 2 (every pose, clashes included): the per-term rule |d| <= 1e-4|ref| + n_terms/1024
+    # in gene units, n_terms = quantised terms feeding a gene (atoms + both ends of every pair)
+    assert np.all(diff <= helpers.gradient_bound(case, gr_ref)), diff.max(axis=0)
     del dj
 
 

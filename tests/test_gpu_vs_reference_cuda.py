@@ -40,8 +40,15 @@ def test_scorer_matches_reference_cuda(case):
     gr_ref = torch.zeros_like(gt)
     assert refpy.cuda_call("score", len(g), gt, e_ref, gr_ref) == 0
     e_ref, gr_ref = e_ref.cpu().numpy(), gr_ref.cpu().numpy()
-    # the reference runs with -use_fast_math (__sinf, __powf, approximate division)
-    assert np.all(np.abs(e_me - e_ref) <= 1e-4 * np.abs(e_ref) + 1e-3)
+    # the reference runs with -use_fast_math (__sinf, __powf, approximate
+    # division): against exact arithmetic (the oracle) its own energies are off
+    # by up to ~1.3e-4 in clashing poses (E > 1e4, where r^-12 amplifies the
+    # __powf error), so the engine is held to 1e-4 there only against the oracle
+    e_or = case.host.score(g, False, nthreads=8)
+    big = np.abs(e_ref) > 1e4
+    assert np.all(np.abs(e_me - e_ref)[~big] <= 1e-4 * np.abs(e_ref[~big]) + 1e-3)
+    assert np.all(np.abs(e_me - e_ref)[big] <= 3e-4 * np.abs(e_ref[big]))
+    assert np.all(np.abs(e_me - e_or) <= 1e-4 * np.abs(e_or) + 1e-3)
     ng = case.ngenes
     bad = np.abs(gr_me[:, :ng] - gr_ref[:, :ng]) > helpers.gradient_tolerance(case, gr_ref)
     assert bad[:, :3].mean() <= 0.002 and bad[:, 6:].mean() <= 0.01 and bad[:, 3:6].mean() <= 0.02
