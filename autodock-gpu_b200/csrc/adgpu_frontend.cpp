@@ -8,9 +8,6 @@ adgpu_status fail(adgpu_status st, const std::string& msg);
 }
 using namespace adgpu;
 
-struct adgpu_grid_s { Grid g; };
-struct adgpu_ligand_s { Prepared p; };
-
 extern "C" {
 
 adgpu_status adgpu_grid_read(const char* fld_path, adgpu_grid** out)

@@ -36,6 +36,14 @@ struct Prepared {
 	std::vector<uint32_t> prng;        // runs * pop_size * 64
 };
 
+}  // namespace adgpu
+
+// The opaque handles of the C ABI.
+struct adgpu_grid_s { adgpu::Grid g; };
+struct adgpu_ligand_s { adgpu::Prepared p; };
+
+namespace adgpu {
+
 adgpu_status grid_read(const char* fld_path, Grid& g);
 void grid_reference_layout(const Grid& g, float* out);      // 4 * nmaps * X*Y*Z floats
 void grid_cell_records(const Grid& g, float* out);          // (X-1)(Y-1)(Z-1) * nmaps * 8 floats

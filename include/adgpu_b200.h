@@ -296,6 +296,65 @@ adgpu_status adgpu_ligand_tables(const adgpu_ligand* lig, adgpu_dockpars* dockpa
 adgpu_status adgpu_ligand_population(const adgpu_ligand* lig, float* initpop, size_t n_floats,
                                      uint32_t* prng, size_t n_states);
 
+/* ---------------------------------------------------------------------------
+ * Layer 2: batch / serving engine (no counterpart in the reference, which
+ * docks one ligand at a time through the layer-1 API).
+ *
+ * Receptor maps stay resident; each submitted request (a prepared ligand
+ * with its runs) keeps its populations, energies, eval counters and PRNG
+ * states on the device until its result is taken.  adgpu_engine_tick
+ * advances every admitted run by up to gens_per_tick generations in one
+ * persistent launch per threads-per-pose class (a CTA carries a run through
+ * whole generations: GA, local search, eval sum, stop test); between ticks
+ * requests can be submitted and results taken (continuous batching).  Each
+ * run stops on its own budget (evals >= max_evals or generations >=
+ * max_gens), so a request's result does not depend on what else is running.
+ * ------------------------------------------------------------------------- */
+typedef struct adgpu_engine_s adgpu_engine;
+
+typedef struct {
+	size_t memory_budget_bytes;  /* device bytes for receptors + requests; 0: 80% of free memory */
+	int    threads_per_pose;     /* 32, 64 or 128; 0: tuned per ligand size class */
+	int    gens_per_tick;        /* generations per tick; <= 0: run every admitted run to completion */
+	int    device;               /* CUDA device ordinal */
+} adgpu_engine_config;
+
+typedef struct {
+	int      receptor;           /* id from adgpu_engine_add_receptor */
+	int      lsmet;              /* 0 sw, 1 ad, 2 adam, 3 fire */
+	uint64_t max_evals;          /* evaluations per run */
+	uint32_t max_gens;           /* generations per run; 0: unlimited */
+} adgpu_request_params;
+
+typedef struct {
+	uint64_t submitted, completed, ticks;
+	size_t   bytes_used, bytes_budget;
+	int      active;
+} adgpu_engine_stats;
+
+adgpu_status adgpu_engine_create(const adgpu_engine_config* cfg, adgpu_engine** out);
+void adgpu_engine_destroy(adgpu_engine* engine);
+/* Uploads a receptor's maps once (8-corner cell records); returns its id. */
+adgpu_status adgpu_engine_add_receptor(adgpu_engine* engine, const adgpu_grid* grid, int* receptor_id);
+/* Admits a request; ADGPU_ERR_BUDGET when its device state does not fit now
+ * (retry after taking results).  The ligand must have been prepared against
+ * a grid equal to the receptor's, with num_runs > 0. */
+adgpu_status adgpu_engine_submit(adgpu_engine* engine, const adgpu_ligand* ligand, const adgpu_request_params* params,
+                                 uint64_t* request_id);
+/* One engine step (see above); *completed = requests finished in it. */
+adgpu_status adgpu_engine_tick(adgpu_engine* engine, int* completed);
+/* Ticks until every admitted request has finished. */
+adgpu_status adgpu_engine_run(adgpu_engine* engine);
+adgpu_status adgpu_engine_poll(adgpu_engine* engine, uint64_t request_id, int* done);
+/* Result of a finished request (any output may be NULL): best energy and
+ * genotype of each run's final population, evals and generations per run,
+ * submit-to-finish latency.  Frees the request's device state. */
+adgpu_status adgpu_engine_result(adgpu_engine* engine, uint64_t request_id, float* best_energies,
+                                 float* best_genotypes, int* evals, uint32_t* generations, double* latency_s);
+adgpu_status adgpu_engine_stats_get(adgpu_engine* engine, adgpu_engine_stats* out);
+/* Threads per pose the engine chose for a request, and its run count. */
+adgpu_status adgpu_engine_request_info(adgpu_engine* engine, uint64_t request_id, int* threads_per_pose, int* runs);
+
 /* Measurement helper (no counterpart in the reference): measured FP32 FMA
  * throughput of the current device in TFLOP/s, the denominator of the
  * scorer's roofline fraction.  device_scratch must hold 2048 floats per SM. */

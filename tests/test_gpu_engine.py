@@ -1,0 +1,123 @@
+"""The batch / serving engine: same results as the plain per-ligand path,
+identical results alone and in a mix, continuous admission, memory budget."""
+import numpy as np
+import pytest
+import torch
+
+from adgpu_b200 import device, dock, engine, frontend, synth
+
+pytestmark = pytest.mark.gpu
+SEED = (305419896, 2271560481, 3735928559)
+
+
+@pytest.fixture(scope="module")
+def grid():
+    spec = synth.grid_spec(40, synth.MAP_TYPES_5, seed=12346)
+    maps = synth.quantize_maps(synth.make_maps(spec))
+    return frontend.Grid.from_maps(maps, synth.MAP_TYPES_5, spec.spacing, spec.origin)
+
+
+def ligand(grid, idx, n_heavy, n_tors, runs=4, pop=150):
+    mol = synth.ligand_for(3, idx, n_heavy, n_tors)
+    text = "\n".join(synth.pdbqt_lines(mol)[0]) + "\n"
+    return frontend.Ligand(grid, text, None, run=frontend.default_dockpars(grid.spacing, pop), seed=SEED,
+                           num_runs=runs)
+
+
+@pytest.mark.parametrize("lsmet", ["ad", "sw"])
+def test_engine_matches_plain_path(grid, lsmet):
+    """With a generation budget both paths stop at the same generation, so every
+    run must come out identical (same kernels, same PRNG states)."""
+    lig = ligand(grid, 0, 16, 4, runs=3)
+    gens = 6
+    # plain: reference kernel API, resident loop
+    job = device.DeviceJob(lig.tables, lig.dockpars, grid.reference_layout(), 3, lig.prng)
+    job.activate()
+    res = dock.dock(job, lig.initpop, lsmet, nev=10**9, ngen=gens)
+    assert res.generations == gens
+    P = lig.dockpars.pop_size
+    e_plain = res.energies.cpu().numpy().reshape(3, P)
+    # engine
+    en = engine.Engine(threads_per_pose=32)
+    rec = en.add_receptor(grid)
+    rid = en.submit(lig, rec, lsmet, max_evals=10**12, max_gens=gens)
+    en.run()
+    r = en.result(rid)
+    assert np.all(r.generations == gens)
+    np.testing.assert_array_equal(r.evals, res.evals_per_run)
+    np.testing.assert_array_equal(r.best_energies, e_plain.min(axis=1))
+
+
+def test_batch_uneven_ligands_and_mix_invariance(grid):
+    sizes = [(12, 0), (16, 4), (24, 8), (30, 12), (20, 6), (40, 16)]
+    ligs = [ligand(grid, i, a, t, runs=3) for i, (a, t) in enumerate(sizes)]
+    nev = 40_000
+    # alone
+    alone = []
+    for lg in ligs[:3]:
+        en = engine.Engine(threads_per_pose=32)
+        rec = en.add_receptor(grid)
+        rid = en.submit(lg, rec, "ad", max_evals=nev)
+        en.run()
+        alone.append(en.result(rid))
+        en.close()
+    # all together in one batch
+    en = engine.Engine(threads_per_pose=32)
+    rec = en.add_receptor(grid)
+    ids = [en.submit(lg, rec, "ad", max_evals=nev) for lg in ligs]
+    en.run()
+    mix = [en.result(i) for i in ids]
+    for a, b in zip(alone, mix[:3]):
+        np.testing.assert_array_equal(a.best_energies, b.best_energies)
+        np.testing.assert_array_equal(a.best_genotypes, b.best_genotypes)
+        np.testing.assert_array_equal(a.evals, b.evals)
+    for lg, r in zip(ligs, mix):
+        assert np.all(r.evals >= nev)
+        e0 = np.array([lg.initpop.shape[0]])  # noqa: F841
+        assert np.all(np.isfinite(r.best_energies))
+        assert r.best_energies.max() < 1e6
+
+
+def test_continuous_admission_and_budget(grid):
+    ligs = [ligand(grid, 10 + i, 14 + 2 * i, 2 + i, runs=2) for i in range(5)]
+    nev = 30_000
+    ref = []
+    for lg in ligs:
+        en = engine.Engine(threads_per_pose=32)
+        rec = en.add_receptor(grid)
+        rid = en.submit(lg, rec, "ad", max_evals=nev)
+        en.run()
+        ref.append(en.result(rid))
+        en.close()
+    # serving: small ticks; requests arrive while others are in flight
+    en = engine.Engine(threads_per_pose=32, gens_per_tick=2)
+    rec = en.add_receptor(grid)
+    pending = list(range(len(ligs)))
+    live, out = {}, {}
+    first = pending.pop(0)
+    live[en.submit(ligs[first], rec, "ad", max_evals=nev)] = first
+    ticks = 0
+    while live or pending:
+        en.tick()
+        ticks += 1
+        if pending and ticks % 2 == 1:
+            k = pending.pop(0)
+            live[en.submit(ligs[k], rec, "ad", max_evals=nev)] = k
+        for rid in [r for r in live if en.done(r)]:
+            out[live.pop(rid)] = en.result(rid)
+    assert ticks > 2
+    for k, r in out.items():
+        np.testing.assert_array_equal(r.best_energies, ref[k].best_energies)
+        np.testing.assert_array_equal(r.evals, ref[k].evals)
+    # a budget too small for a second request is refused, and admitted after a result is taken
+    small = engine.Engine(threads_per_pose=32, memory_budget_bytes=64 << 20)
+    rec = small.add_receptor(grid)
+    a = small.submit(ligs[0], rec, "ad", max_evals=nev)
+    n = 1
+    while small.submit(ligs[1], rec, "ad", max_evals=nev, raise_on_budget=False) is not None:
+        n += 1
+        assert n < 1000
+    small.run()
+    small.result(a)
+    assert small.submit(ligs[1], rec, "ad", max_evals=nev, raise_on_budget=False) is not None
+    torch.cuda.synchronize()
