@@ -87,6 +87,42 @@ def make_maps(spec: GridSpec) -> dict:
     return out
 
 
+def make_maps_fast(spec: GridSpec, device: str = "cuda") -> dict:
+    """make_maps computed with torch on `device` (float64): the same field,
+    seconds instead of minutes for 100^3 grids.  Values agree with make_maps
+    to rounding, not bit for bit; benchmarks use it for large receptors."""
+    import torch
+    rng = np.random.default_rng(spec.seed)
+    rec = (rng.random((spec.n_rec_atoms, 3)) - 0.5) * spec.rec_box + np.asarray(spec.center)
+    rec_q = rng.normal(0.0, 0.3, spec.n_rec_atoms)
+    nx, ny, nz = spec.dims
+    ox, oy, oz = spec.origin
+    dev = torch.device(device)
+    rec_t = torch.tensor(rec, dtype=torch.float64, device=dev)
+    q_t = torch.tensor(rec_q, dtype=torch.float64, device=dev)
+    xs = ox + spec.spacing * torch.arange(nx, dtype=torch.float64, device=dev)
+    ys = oy + spec.spacing * torch.arange(ny, dtype=torch.float64, device=dev)
+    zs = oz + spec.spacing * torch.arange(nz, dtype=torch.float64, device=dev)
+    out = {t: np.empty((nz, ny, nx), np.float32) for t in list(spec.types) + ["e", "d"]}
+    gy, gx = torch.meshgrid(ys, xs, indexing="ij")
+    px, py = gx.reshape(-1, 1), gy.reshape(-1, 1)
+    for iz in range(nz):
+        d2 = (px - rec_t[None, :, 0]) ** 2 + (py - rec_t[None, :, 1]) ** 2 + (zs[iz] - rec_t[None, :, 2]) ** 2
+        r = torch.sqrt(torch.clamp(d2, min=1e-4))
+        for t in spec.types:
+            rii, eii = _MAP_TYPE_PARAMS.get(t, (3.5, 0.15))
+            rij = 0.5 * (rii + _REC_R)
+            eij = math.sqrt(eii * _REC_EPS)
+            x6 = (rij / r) ** 6
+            v = (eij * (x6 * x6 - 2.0 * x6)).sum(dim=1)
+            out[t][iz] = torch.clamp(v, -2.0, 1e5).reshape(ny, nx).float().cpu().numpy()
+        e = (_ELEC * q_t[None, :] / (4.0 * r * r)).sum(dim=1)
+        out["e"][iz] = torch.clamp(e, -2.0, 1e5).reshape(ny, nx).float().cpu().numpy()
+        dsol = (0.01097 * 12.0 * torch.exp(-d2 / (2.0 * 3.6 * 3.6))).sum(dim=1)
+        out["d"][iz] = torch.clamp(dsol, -2.0, 1e5).reshape(ny, nx).float().cpu().numpy()
+    return out
+
+
 def write_maps(spec: GridSpec, maps: dict, directory: str, name: str = "receptor") -> str:
     """Writes name.maps.fld and name.<type>.map files; returns the .fld path."""
     os.makedirs(directory, exist_ok=True)
@@ -203,8 +239,9 @@ def make_ligand(seed: int, n_heavy: int, n_torsions: int,
             continue
         bonds = [(parent[i], i) for i in range(1, n_heavy)]
         internal = [(a, b) for (a, b) in bonds if deg[a] > 1 and deg[b] > 1]
-        if len(internal) < n_torsions:
+        if len(internal) < n_torsions and _attempt < 50:
             continue
+        n_torsions = min(n_torsions, len(internal))   # small trees cannot hold every requested torsion
         break
     else:
         raise RuntimeError("could not build ligand")

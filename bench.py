@@ -378,6 +378,131 @@ def run_kernel_only(args):
                       "evals_last_launch": int(job.evals_new.sum().item())}))
 
 
+def _ligand_text(config_id, idx, n_heavy, n_tors, types=None):
+    from adgpu_b200 import synth
+    mol = synth.ligand_for(config_id, idx, n_heavy, n_tors, types=types)
+    return "\n".join(synth.pdbqt_lines(mol)[0]) + "\n"
+
+
+def run_batch(args):
+    """--mode batch: uneven ligands docked by the batch engine (all ligands and
+    runs in one persistent launch per threads-per-pose class) next to plain
+    per-ligand dockings through the reference kernel API, same ligands, same
+    budget.  A bounded sample of the batching configuration (1024 ligands,
+    10-64 heavy atoms, 0-32 torsions, nrun 20, 2.5M evals per run)."""
+    import torch
+    from adgpu_b200 import device, dock, engine, frontend, synth
+    w = WORKLOAD
+    spec = synth.grid_spec(w["npts"], w["types"], seed=12345 + 3)
+    grid = frontend.Grid.from_maps(synth.quantize_maps(synth.make_maps_fast(spec)), w["types"], spec.spacing, spec.origin)
+    rng = np.random.default_rng(3)
+    nlig, nrun, nev = args.nlig, 20, args.nev
+    sizes = [(int(rng.integers(10, 65)), int(rng.integers(0, 33))) for _ in range(nlig)]
+    run = frontend.default_dockpars(grid.spacing, 150)
+    ligs = [frontend.Ligand(grid, _ligand_text(3, i, a, t), None, run=run, seed=w["seed"], num_runs=nrun)
+            for i, (a, t) in enumerate(sizes)]
+    # batched: one engine, everything admitted, run to completion
+    en = engine.Engine(threads_per_pose=args.tpp if args.tpp != 32 else 0)
+    rec = en.add_receptor(grid)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ids = [en.submit(lg, rec, args.lsmet, max_evals=nev) for lg in ligs]
+    en.run()
+    res = [en.result(i) for i in ids]
+    t_batch = time.perf_counter() - t0
+    ev_batch = sum(int(r.evals.sum()) for r in res)
+    tpps = {}
+    # plain: one ligand at a time (the reference's way of driving the same kernels)
+    nplain = min(nlig, args.plain_sample)
+    ref_grid = grid.reference_layout()
+    t_plain, ev_plain = 0.0, 0
+    for lg in ligs[:nplain]:
+        job = device.DeviceJob(lg.tables, lg.dockpars, ref_grid, nrun, lg.prng)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        job.activate()
+        r = dock.dock(job, lg.initpop, args.lsmet, nev, 42000)
+        torch.cuda.synchronize()
+        t_plain += time.perf_counter() - t0
+        ev_plain += int(r.evals_per_run.sum())
+        del job
+    lph_b = 3600.0 * nlig / t_batch
+    lph_p = 3600.0 * nplain / t_plain
+    return {"mode": "batch", "ligands": nlig, "nrun": nrun, "nev_per_run": nev, "lsmet": args.lsmet,
+            "heavy_atoms": [min(a for a, _ in sizes), max(a for a, _ in sizes)],
+            "batched": {"seconds": t_batch, "ligands_per_hour": lph_b, "evals_per_s": ev_batch / t_batch},
+            "plain": {"ligands_sampled": nplain, "seconds": t_plain, "ligands_per_hour": lph_p,
+                      "evals_per_s": ev_plain / t_plain},
+            "batched_over_plain_ligands_per_hour": lph_b / lph_p, "tpp_classes": tpps}
+
+
+def run_serve(args):
+    """--mode serve: a Poisson stream of cfg2-sized requests against three
+    resident receptors (60^3, 80^3, 100^3 maps, 7 types + e + d), arrival rate
+    80% of the measured batched capacity, admission by a fixed device-memory
+    budget; p50/p99 request latency (arrival to result) and ligands/hour."""
+    import torch
+    from adgpu_b200 import engine, frontend, synth
+    w = WORKLOAD
+    types = synth.MAP_TYPES_7
+    grids = []
+    for k, n in enumerate((60, 80, 100)):
+        spec = synth.grid_spec(n, types, seed=12345 + 5 + k)
+        grids.append(frontend.Grid.from_maps(synth.quantize_maps(synth.make_maps_fast(spec)), types, spec.spacing,
+                                             spec.origin))
+    nrun, nev, nreq = 10, args.nev, args.nreq
+    ltypes = (("C", 0.55), ("A", 0.15), ("N", 0.08), ("NA", 0.04), ("OA", 0.13), ("SA", 0.05))
+    rng = np.random.default_rng(5)
+    texts = [_ligand_text(5, i, 40, 10, types=ltypes) for i in range(nreq)]
+    targets = [int(rng.integers(0, 3)) for _ in range(nreq)]
+    ligs = [frontend.Ligand(grids[t], texts[i], None, run=frontend.default_dockpars(grids[t].spacing, 150),
+                            seed=w["seed"], num_runs=nrun) for i, t in enumerate(targets)]
+    budget = args.budget_gb << 30
+    # capacity: a batch of requests run to completion
+    cap_n = min(nreq, 48)
+    en = engine.Engine(memory_budget_bytes=budget, gens_per_tick=4)
+    recs = [en.add_receptor(g) for g in grids]
+    t0 = time.perf_counter()
+    ids = [en.submit(ligs[i], recs[targets[i]], args.lsmet, max_evals=nev) for i in range(cap_n)]
+    en.run()
+    for i in ids:
+        en.result(i)
+    capacity = cap_n / (time.perf_counter() - t0)          # ligands / s
+    rate = 0.8 * capacity
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    # serving loop
+    t_start = time.perf_counter()
+    pending, live, lat, queued = list(range(nreq)), {}, [], []
+    done_n = 0
+    while done_n < nreq:
+        now = time.perf_counter() - t_start
+        while pending and arrivals[pending[0]] <= now:
+            queued.append(pending.pop(0))
+        while queued:
+            i = queued[0]
+            rid = en.submit(ligs[i], recs[targets[i]], args.lsmet, max_evals=nev, raise_on_budget=False)
+            if rid is None:
+                break
+            live[rid] = i
+            queued.pop(0)
+        if live:
+            en.tick()
+            for rid in [r for r in live if en.done(r)]:
+                i = live.pop(rid)
+                en.result(rid)
+                lat.append(time.perf_counter() - t_start - arrivals[i])
+                done_n += 1
+        else:
+            time.sleep(0.001)
+    t_total = time.perf_counter() - t_start
+    torch.cuda.synchronize()
+    lat = np.array(lat)
+    return {"mode": "serve", "requests": nreq, "nrun": nrun, "nev_per_run": nev, "receptors": "60^3, 80^3, 100^3",
+            "batched_capacity_ligands_per_s": capacity, "arrival_rate_per_s": rate,
+            "ligands_per_hour": 3600.0 * nreq / t_total, "latency_p50_s": float(np.percentile(lat, 50)),
+            "latency_p99_s": float(np.percentile(lat, 99)), "memory_budget_gb": args.budget_gb}
+
+
 def _hbm_peak():
     try:
         return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
@@ -393,12 +518,21 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--lsmet", default="ad", choices=["ad", "sw", "adam", "fire"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel"])
+    ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel", "batch", "serve"])
     ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel mode)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
+    ap.add_argument("--nlig", type=int, default=64, help="ligands (batch mode)")
+    ap.add_argument("--nev", type=int, default=250_000, help="evaluations per run (batch / serve modes)")
+    ap.add_argument("--plain-sample", type=int, default=16, help="ligands docked one at a time for the plain arm")
+    ap.add_argument("--nreq", type=int, default=200, help="requests (serve mode)")
+    ap.add_argument("--budget-gb", type=int, default=8, help="engine device-memory budget (serve mode)")
     args = ap.parse_args()
     if args.mode == "ls-kernel":
         run_kernel_only(args)
+        return
+    if args.mode in ("batch", "serve"):
+        out = run_batch(args) if args.mode == "batch" else run_serve(args)
+        print(json.dumps(out), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
