@@ -25,6 +25,39 @@ class DockResult:
     generations: int
 
 
+def dock_host_loop(job: DeviceJob, initpop: np.ndarray | torch.Tensor, lsmet: str = "ad", nev: int = 2_500_000,
+                   ngen: int = 42_000) -> DockResult:
+    """The reference host's own generation loop (docking_with_gpu,
+    host/src/performdocking.cpp.Cuda:640-831) over the kernel API: one
+    synchronous call per kernel per generation and a host-side progress check
+    on the per-run eval counters -- how a drop-in user drives the kernels."""
+    R, P = job.runs, job.dp.pop_size
+    cur, ecur = job.population()
+    nxt, enxt = job.population()
+    cur.copy_(initpop[:R * P] if isinstance(initpop, torch.Tensor)
+              else torch.from_numpy(np.ascontiguousarray(initpop[:R * P], np.float32)))
+    job.evals_runs.zero_()
+    T = REF_THREADS
+    lib.call("adgpu_calc_initpop", R * P, T, cur, ecur)
+    lib.call("adgpu_sum_evals", R, T)
+    ls = {"sw": "adgpu_perform_ls", "ad": "adgpu_gradient_minad", "adam": "adgpu_gradient_minadam",
+          "fire": "adgpu_gradient_minfire"}[lsmet]
+    L = job.dp.num_of_lsentities
+    gen = 0
+    while True:
+        total = int(job.evals_runs.sum().item())                  # check_progress (:908-942)
+        progress = max(total / R / nev * 100.0, gen / ngen * 100.0)
+        if progress >= 100.0:
+            break
+        lib.call("adgpu_gen_and_eval_newpops", R * P, T, cur, ecur, nxt, enxt)
+        lib.call(ls, R * L, T, nxt, enxt)
+        lib.call("adgpu_sum_evals", R, T)
+        gen += 1
+        cur, nxt = nxt, cur
+        ecur, enxt = enxt, ecur
+    return DockResult(cur, ecur, job.evals_runs.cpu().numpy().copy(), gen)
+
+
 def dock(job: DeviceJob, initpop: np.ndarray | torch.Tensor, lsmet: str = "ad", nev: int = 2_500_000,
          ngen: int = 42_000, buffers=None) -> DockResult:
     """Docks the active ligand: runs*pop entities from `initpop`, until the

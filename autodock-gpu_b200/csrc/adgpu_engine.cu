@@ -51,13 +51,18 @@ struct ReqDev {
 
 struct RunRef { int req; int run; };
 
-constexpr int kEngineThreads = 256;
+// 128-thread CTAs, several per SM: a CTA waits at the end of a generation's
+// local search for its slowest entity, and other CTAs' runs fill the SM then.
+constexpr int kEngineThreads = 128;
+#ifndef ADGPU_ENGINE_MIN_CTAS
+#define ADGPU_ENGINE_MIN_CTAS 6
+#endif
 
 // --------------------------------------------------------------------------
-// the engine kernel
+// the engine kernel (one instantiation per threads-per-pose x local search)
 // --------------------------------------------------------------------------
-template <int TPP>
-__global__ void __launch_bounds__(kEngineThreads, 2)
+template <int TPP, int LSMET>
+__global__ void __launch_bounds__(kEngineThreads, ADGPU_ENGINE_MIN_CTAS)
 engine_kernel(const ReqDev* __restrict__ reqs, const RunRef* __restrict__ work, uint8_t* work_done, int nwork, int gens_per_tick,
               unsigned int* counter, int max_atoms, int max_tors)
 {
@@ -106,9 +111,9 @@ engine_kernel(const ReqDev* __restrict__ reqs, const RunRef* __restrict__ work, 
 			const int c = rq.cur[run];
 			if (!rq.init[run]) {
 				// initial population of this run (cuda/kernel1.cu:26-55)
-				KArgs a = sa;
-				a.conf = rq.conf[c]; a.e = rq.e[c];
-				for (int e = local; e < P; e += gpc) initpop_block<TPP>(a, (uint32_t)(run * P + e), G, S);
+				if (threadIdx.x == 0) { sa.conf = rq.conf[c]; sa.e = rq.e[c]; }
+				__syncthreads();
+				for (int e = local; e < P; e += gpc) initpop_block<TPP>(sa, (uint32_t)(run * P + e), G, S);
 				__syncthreads();
 				if (threadIdx.x == 0) { rq.init[run] = 1; rq.evals_runs[run] = P; }
 				__syncthreads();
@@ -116,16 +121,17 @@ engine_kernel(const ReqDev* __restrict__ reqs, const RunRef* __restrict__ work, 
 			}
 			// GA generation (cuda/kernel4.cu): current -> next
 			{
-				KArgs a = sa;
-				a.conf_cur = rq.conf[c]; a.e_cur = rq.e[c];
-				a.conf = rq.conf[c ^ 1]; a.e = rq.e[c ^ 1];
-				for (int e = local; e < P; e += gpc) ga_block<TPP>(a, (uint32_t)(run * P + e), G, S);
+				if (threadIdx.x == 0) {
+					sa.conf_cur = rq.conf[c]; sa.e_cur = rq.e[c];
+					sa.conf = rq.conf[c ^ 1]; sa.e = rq.e[c ^ 1];
+				}
+				__syncthreads();
+				for (int e = local; e < P; e += gpc) ga_block<TPP>(sa, (uint32_t)(run * P + e), G, S);
 			}
 			__syncthreads();
 			// local search on the next population, entities taken dynamically
 			if (sa.dp.lsearch_rate != 0.0f) {
-				KArgs a = sa;
-				a.conf = rq.conf[c ^ 1]; a.e = rq.e[c ^ 1];
+				const KArgs& a = sa;          // conf/e already point at the next population
 				for (;;) {
 					uint32_t l = 0;
 					if (G.rank == 0) l = (uint32_t)atomicAdd(&s_ls, 1);
@@ -138,12 +144,10 @@ engine_kernel(const ReqDev* __restrict__ reqs, const RunRef* __restrict__ work, 
 					}
 					if (l >= L) break;
 					const uint32_t b = (uint32_t)run * L + l;
-					switch (rq.lsmet) {
-					case LS_SW: sw_block<TPP>(a, b, G, S); break;
-					case LS_AD: gradient_ls_block<TPP, LS_AD>(a, b, G, S); break;
-					case LS_ADAM: gradient_ls_block<TPP, LS_ADAM>(a, b, G, S); break;
-					default: fire_block<TPP>(a, b, G, S); break;
-					}
+					if constexpr (LSMET == LS_SW) sw_block<TPP>(a, b, G, S);
+					else if constexpr (LSMET == LS_AD) gradient_ls_block<TPP, LS_AD>(a, b, G, S);
+					else if constexpr (LSMET == LS_ADAM) gradient_ls_block<TPP, LS_ADAM>(a, b, G, S);
+					else fire_block<TPP>(a, b, G, S);
 				}
 			}
 			__syncthreads();
@@ -262,11 +266,11 @@ static size_t request_bytes(int runs, int pop, size_t tables)
 	       (size_t)runs * (4 + 4 + 3 + 4 + kGenotypeStride * 4) + 1024;
 }
 
-template <int TPP>
+template <int TPP, int LSMET>
 static adgpu_status launch_engine(Engine& E, const RunRef* work, uint8_t* work_done, int nwork, int gens, int max_atoms, int max_tors, unsigned int* counter)
 {
 	const int bytes = group_smem_bytes(max_atoms, max_tors, 64, TPP) * (kEngineThreads / TPP);
-	auto k = engine_kernel<TPP>;
+	auto k = engine_kernel<TPP, LSMET>;
 	if (bytes > 48 * 1024) {
 		cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 		if (e != cudaSuccess) return cuda_fail(e, "engine smem");
@@ -440,12 +444,14 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	// active requests and their runs, grouped by threads-per-pose class
 	std::vector<ReqDev> reqs;
 	std::vector<Request*> order;
-	std::vector<RunRef> work[3];
-	int max_atoms[3] = {1, 1, 1}, max_tors[3] = {0, 0, 0};
+	constexpr int NC = 12;                 // classes: threads per pose (3) x local search (4)
+	std::vector<RunRef> work[NC];
+	int max_atoms[NC], max_tors[NC];
+	for (int c = 0; c < NC; c++) { max_atoms[c] = 1; max_tors[c] = 0; }
 	for (auto& kv : E.requests) {
 		Request& r = *kv.second;
 		if (r.done) continue;
-		int cls = r.tpp == 32 ? 0 : (r.tpp == 64 ? 1 : 2);
+		int cls = (r.tpp == 32 ? 0 : (r.tpp == 64 ? 1 : 2)) * 4 + r.dev.lsmet;
 		int idx = (int)reqs.size();
 		reqs.push_back(r.dev);
 		order.push_back(&r);
@@ -455,7 +461,8 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	}
 	if (completed) *completed = 0;
 	if (reqs.empty()) return ADGPU_OK;
-	size_t nwork = work[0].size() + work[1].size() + work[2].size();
+	size_t nwork = 0;
+	for (int c = 0; c < NC; c++) nwork += work[c].size();
 	cudaError_t e;
 	if ((int)reqs.size() > E.d_reqs_cap) {
 		if (E.d_reqs) cudaFree(E.d_reqs);
@@ -471,23 +478,29 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	}
 	std::vector<RunRef> all;
 	all.reserve(nwork);
-	size_t start[3];
-	for (int c = 0; c < 3; c++) { start[c] = all.size(); all.insert(all.end(), work[c].begin(), work[c].end()); }
+	size_t start[NC];
+	for (int c = 0; c < NC; c++) { start[c] = all.size(); all.insert(all.end(), work[c].begin(), work[c].end()); }
 	uint8_t* d_done = reinterpret_cast<uint8_t*>(E.d_work + E.d_work_cap);
 	e = cudaMemcpyAsync(E.d_reqs, reqs.data(), sizeof(ReqDev) * reqs.size(), cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_work, all.data(), sizeof(RunRef) * nwork, cudaMemcpyHostToDevice, E.stream);
-	if (e == cudaSuccess) e = cudaMemsetAsync(E.d_counters, 0, 3 * sizeof(unsigned int), E.stream);
+	if (e == cudaSuccess) e = cudaMemsetAsync(E.d_counters, 0, NC * sizeof(unsigned int), E.stream);
 	if (e != cudaSuccess) return cuda_fail(e, "tick upload");
 	const int gens = E.cfg.gens_per_tick;
-	for (int c = 0; c < 3; c++) {
+	for (int c = 0; c < NC; c++) {
 		if (work[c].empty()) continue;
-		adgpu_status st;
+		adgpu_status st = ADGPU_OK;
 		const RunRef* w = E.d_work + start[c];
 		uint8_t* wd = d_done + start[c];
 		int n = (int)work[c].size();
-		if (c == 0) st = launch_engine<32>(E, w, wd, n, gens, max_atoms[c], max_tors[c], E.d_counters + c);
-		else if (c == 1) st = launch_engine<64>(E, w, wd, n, gens, max_atoms[c], max_tors[c], E.d_counters + c);
-		else st = launch_engine<128>(E, w, wd, n, gens, max_atoms[c], max_tors[c], E.d_counters + c);
+		unsigned int* ctr = E.d_counters + c;
+#define ADGPU_ENGINE_CASE(ID, TPP, LS) \
+		case ID: st = launch_engine<TPP, LS>(E, w, wd, n, gens, max_atoms[c], max_tors[c], ctr); break;
+		switch (c) {
+			ADGPU_ENGINE_CASE(0, 32, LS_SW) ADGPU_ENGINE_CASE(1, 32, LS_AD) ADGPU_ENGINE_CASE(2, 32, LS_ADAM) ADGPU_ENGINE_CASE(3, 32, LS_FIRE)
+			ADGPU_ENGINE_CASE(4, 64, LS_SW) ADGPU_ENGINE_CASE(5, 64, LS_AD) ADGPU_ENGINE_CASE(6, 64, LS_ADAM) ADGPU_ENGINE_CASE(7, 64, LS_FIRE)
+			ADGPU_ENGINE_CASE(8, 128, LS_SW) ADGPU_ENGINE_CASE(9, 128, LS_AD) ADGPU_ENGINE_CASE(10, 128, LS_ADAM) ADGPU_ENGINE_CASE(11, 128, LS_FIRE)
+		}
+#undef ADGPU_ENGINE_CASE
 		if (st != ADGPU_OK) return st;
 	}
 	E.h_done.resize(nwork);

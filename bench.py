@@ -412,28 +412,33 @@ def run_batch(args):
     t_batch = time.perf_counter() - t0
     ev_batch = sum(int(r.evals.sum()) for r in res)
     tpps = {}
-    # plain: one ligand at a time (the reference's way of driving the same kernels)
+    # plain: one ligand at a time through the kernel API, (a) driven by the
+    # reference host's loop (a synchronous call per kernel per generation) --
+    # the drop-in -- and (b) with the loop resident on the device
     nplain = min(nlig, args.plain_sample)
     ref_grid = grid.reference_layout()
-    t_plain, ev_plain = 0.0, 0
-    for lg in ligs[:nplain]:
-        job = device.DeviceJob(lg.tables, lg.dockpars, ref_grid, nrun, lg.prng)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        job.activate()
-        r = dock.dock(job, lg.initpop, args.lsmet, nev, 42000)
-        torch.cuda.synchronize()
-        t_plain += time.perf_counter() - t0
-        ev_plain += int(r.evals_per_run.sum())
-        del job
+    plain = {}
+    for name, fn in (("reference_host_loop", dock.dock_host_loop), ("resident_loop", dock.dock)):
+        t_plain, ev_plain = 0.0, 0
+        for lg in ligs[:nplain]:
+            job = device.DeviceJob(lg.tables, lg.dockpars, ref_grid, nrun, lg.prng)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            job.activate()
+            r = fn(job, lg.initpop, args.lsmet, nev, 42000)
+            torch.cuda.synchronize()
+            t_plain += time.perf_counter() - t0
+            ev_plain += int(r.evals_per_run.sum())
+            del job
+        plain[name] = {"ligands_sampled": nplain, "seconds": t_plain, "ligands_per_hour": 3600.0 * nplain / t_plain,
+                       "evals_per_s": ev_plain / t_plain}
     lph_b = 3600.0 * nlig / t_batch
-    lph_p = 3600.0 * nplain / t_plain
     return {"mode": "batch", "ligands": nlig, "nrun": nrun, "nev_per_run": nev, "lsmet": args.lsmet,
             "heavy_atoms": [min(a for a, _ in sizes), max(a for a, _ in sizes)],
             "batched": {"seconds": t_batch, "ligands_per_hour": lph_b, "evals_per_s": ev_batch / t_batch},
-            "plain": {"ligands_sampled": nplain, "seconds": t_plain, "ligands_per_hour": lph_p,
-                      "evals_per_s": ev_plain / t_plain},
-            "batched_over_plain_ligands_per_hour": lph_b / lph_p, "tpp_classes": tpps}
+            "plain": plain,
+            "batched_over_plain_ligands_per_hour": {k: lph_b / v["ligands_per_hour"] for k, v in plain.items()},
+            "tpp_classes": tpps}
 
 
 def run_serve(args):
