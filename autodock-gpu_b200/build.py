@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib", "libadgpu_b200.so")
-SOURCES = ["adgpu_api.cu", "adgpu_tables.cu", "adgpu_engine.cu", "adgpu_compat.cu", "adgpu_prep.cpp", "adgpu_frontend.cpp", "adgpu_probe.cu"]
+SOURCES = ["adgpu_api.cu", "adgpu_tables.cu", "adgpu_engine.cu", "adgpu_compat.cu", "adgpu_prep.cpp", "adgpu_frontend.cpp", "adgpu_probe.cu", "adgpu_noalloc.cu"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-warn-spills"]
 

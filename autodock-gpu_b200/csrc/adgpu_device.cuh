@@ -242,7 +242,10 @@ __device__ __forceinline__ GenRot genrot_of(const float* g, bool has_ligand)
 // Scores genotype g (shared memory, read-only here).  Returns the energy (same
 // value in every thread of the group).  With GRAD, writes dE/dgene to
 // grad[0..ngenes) (shared memory).  Leaves the pose coordinates in S.
-template <int TPP, bool GRAD>
+// REF_GRID: L.grid is the reference's own layout (4 replicated floats per
+// point and map, host/src/processgrid.cpp:244-248) instead of cell records;
+// the same 8 corner values are read, from two 16-byte loads per map.
+template <int TPP, bool GRAD, bool REF_GRID = false>
 __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float* __restrict__ grad,
                            const PoseSmem& S, const Group<TPP>& G)
 {
@@ -296,15 +299,26 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 				fx = fy = fz = kOutOfGridForce;
 			} else {
 				float xl = floorf(x), yl = floorf(y), zl = floorf(z);
-				int cell = (int)xl + (int)yl * L.cells_x + (int)zl * L.cells_xy;
-				const float4* rec = reinterpret_cast<const float4*>(L.grid + (size_t)cell * L.rec_floats);
 				float dx = x - xl, omdx = 1.0f - dx, dy = y - yl, omdy = 1.0f - dy, dz = z - zl, omdz = 1.0f - dz;
 				float w0 = omdx * omdy * omdz, w1 = omdx * dy * omdz, w2 = omdx * omdy * dz, w3 = omdx * dy * dz;
 				float w4 = dx * omdy * omdz, w5 = dx * dy * omdz, w6 = dx * omdy * dz, w7 = dx * dy * dz;
 				int slot = info & 0xFFu;
-				float4 t0 = __ldg(rec + 2 * slot), t1 = __ldg(rec + 2 * slot + 1);
-				float4 e0 = __ldg(rec + 0), e1 = __ldg(rec + 1);
-				float4 d0 = __ldg(rec + 2), d1 = __ldg(rec + 3);
+				float4 t0, t1, e0, e1, d0, d1;
+				if constexpr (REF_GRID) {
+					const size_t g3 = (size_t)L.gx * L.gy * L.gz;
+					const size_t p = (size_t)xl + (size_t)yl * L.gx + (size_t)zl * L.gx * L.gy;
+					const size_t M = (size_t)(L.rec_floats / 8 - 2);
+					const float4* tp = reinterpret_cast<const float4*>(L.grid + ((((size_t)slot - 2) * g3 + p) << 2));
+					const float4* ep = reinterpret_cast<const float4*>(L.grid + ((M * g3 + p) << 2));
+					const float4* dp = reinterpret_cast<const float4*>(L.grid + (((M + 1) * g3 + p) << 2));
+					t0 = __ldg(tp); t1 = __ldg(tp + 1); e0 = __ldg(ep); e1 = __ldg(ep + 1); d0 = __ldg(dp); d1 = __ldg(dp + 1);
+				} else {
+					int cell = (int)xl + (int)yl * L.cells_x + (int)zl * L.cells_xy;
+					const float4* rec = reinterpret_cast<const float4*>(L.grid + (size_t)cell * L.rec_floats);
+					t0 = __ldg(rec + 2 * slot); t1 = __ldg(rec + 2 * slot + 1);
+					e0 = __ldg(rec + 0); e1 = __ldg(rec + 1);
+					d0 = __ldg(rec + 2); d1 = __ldg(rec + 3);
+				}
 				float vt = t0.x * w0 + t0.y * w1 + t0.z * w2 + t0.w * w3 + t1.x * w4 + t1.y * w5 + t1.z * w6 + t1.w * w7;
 				float ve = e0.x * w0 + e0.y * w1 + e0.z * w2 + e0.w * w3 + e1.x * w4 + e1.y * w5 + e1.z * w6 + e1.w * w7;
 				float vd = d0.x * w0 + d0.y * w1 + d0.z * w2 + d0.w * w3 + d1.x * w4 + d1.y * w5 + d1.z * w6 + d1.w * w7;

@@ -229,6 +229,24 @@ adgpu_status adgpu_gradient_minfire(uint32_t blocks, uint32_t threads,
 adgpu_status adgpu_score_genotypes(uint32_t n, const float* genotypes,
                                    float* energies, float* gradients);
 
+/* The same scoring as adgpu_score_genotypes, for callers that may not
+ * allocate device memory: a host whose memory is all handed out by its own
+ * pool, or a process with every byte of the device already reserved.  It has
+ * no counterpart in the reference.  It takes the reference-layout GpuData
+ * directly (adgpu_set_kernels_gpu_data is not needed) and repacks its tables
+ * on the device into one fixed 1 MiB device array compiled into the library,
+ * reading the grid in the caller's layout; it calls neither cudaMalloc nor
+ * cudaFree.  Ligands whose repacked tables exceed 1 MiB (about 30,000
+ * intramolecular pairs) are rejected with ADGPU_ERR_LIMIT.  The first call
+ * on a device looks up that array's device address (cudaGetSymbolAddress),
+ * so make it before any stream capture.  There is one array per device:
+ * calls that overlap on the GPU (from several host threads) race on it.
+ * Runs on the legacy default stream and returns after the scores are
+ * written. */
+adgpu_status adgpu_score_genotypes_noalloc(const adgpu_gpudata* data, uint32_t n,
+                                           const float* genotypes, float* energies,
+                                           float* gradients);
+
 /* Device-resident docking loop for one ligand: the generation loop of
  * docking_with_gpu (host/src/performdocking.cpp.Cuda:684-831) without host
  * round trips.  Runs generations (GA + the LS method `lsmet`: 0 sw, 1 ad,
