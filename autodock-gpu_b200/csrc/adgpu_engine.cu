@@ -4,12 +4,14 @@
 // against device-resident receptor maps.  A request's populations, energies,
 // eval counters and PRNG states live on the device from submission to
 // completion.  The engine advances all admitted runs with one persistent
-// kernel per threads-per-pose class: a CTA takes a run from a work list and
-// carries it through whole generations (initial population, GA, local
-// search, eval sum, stop test) with no grid-wide synchronisation -- runs are
-// independent, as in the reference (one population per run).  A tick
-// advances every run by up to `gens_per_tick` generations; between ticks the
-// host retires finished requests and admits new ones (continuous batching).
+// kernel per local-search method whose pose groups are workers on task
+// queues: every phase of a run (initial population, GA generation, local
+// search) is split into independent tasks, and the group that finishes a
+// phase's last task takes the eval sum and the stop test and queues the run's
+// next phase -- no grid-wide synchronisation; runs are independent, as in the
+// reference (one population per run).  A tick advances every run by up to
+// `gens_per_tick` generations; between ticks the host retires finished
+// requests and admits new ones (continuous batching).
 //
 // Semantics per run follow the reference kernels operation by operation; the
 // one deliberate difference from docking_with_gpu is the stop test, taken
@@ -51,155 +53,311 @@ struct ReqDev {
 
 struct RunRef { int req; int run; };
 
-// 128-thread CTAs, several per SM: a CTA waits at the end of a generation's
-// local search for its slowest entity, and other CTAs' runs fill the SM then.
+// 128-thread CTAs, several per SM; every pose group of a CTA is an
+// independent worker.
 constexpr int kEngineThreads = 128;
 #ifndef ADGPU_ENGINE_MIN_CTAS
 #define ADGPU_ENGINE_MIN_CTAS 6
 #endif
 
 // --------------------------------------------------------------------------
-// the engine kernel (one instantiation per threads-per-pose x local search)
+// task queue
 // --------------------------------------------------------------------------
+// A run advances through phases -- initial population, GA generation, local
+// search -- and each phase is split into independent tasks: a chunk of GA
+// (or initial-population) entities, or one local-search entity.  Tasks of a
+// class (threads per pose) go through one FIFO ring; the pose group that
+// completes the last task of a phase finalises it (eval sum, stop test) and
+// pushes the run's next tasks.  A generation's local searches therefore run
+// on as many pose groups as the run has local-search entities, and no group
+// waits for another run's slowest entity.
+enum : uint32_t { kTaskStart = 0, kTaskInit = 1, kTaskGA = 2, kTaskLS = 3 };
+constexpr uint32_t kTaskIdxBits = 11;                          // entity / chunk index < 2048
+constexpr uint32_t kMaxTickRuns = 1u << (32 - kTaskIdxBits - 2); // run index bits
+constexpr int kSlotSpin = 1 << 20;                             // wait for a reserved slot's write
+constexpr long long kIdleNs = 20000000;                        // an idle worker retires after 20 ms
+
+__host__ __device__ constexpr uint32_t task_word(uint32_t w, uint32_t kind, uint32_t idx)
+{
+	return (w << (kTaskIdxBits + 2)) | (kind << kTaskIdxBits) | idx;
+}
+
+struct QueueCtl {
+	unsigned long long head;    // next position to pop
+	unsigned long long tail;    // next position to push
+	int alive;                  // runs of the class not yet retired in this tick
+	int err;                    // nonzero: a reserved slot was never written
+	int pad[2];
+};
+
+struct TickClass {
+	unsigned long long* slots;  // ring: (lap << 32) | task word, lap = position / cap + 1
+	QueueCtl* ctl;
+	uint32_t cap;
+	int cta_end;                // this class's CTAs are [previous class's cta_end, cta_end)
+	int group_bytes;            // shared memory per pose group
+};
+
+struct TickArgs {
+	const ReqDev* reqs;
+	const RunRef* work;
+	uint8_t* work_done;         // per work item: run finished (written when it retires)
+	int* pending;               // per work item: tasks of the current phase not yet done
+	int* quota;                 // per work item: phases this tick may still run
+	int ga_chunk;               // entities per GA / initial-population task
+	TickClass cls[3];           // threads per pose 32, 64, 128
+};
+
+// Per-pose-group header in shared memory, ahead of the group's scratch.
+struct GroupHdr {
+	KArgs a;                    // the current request's arguments, pointers set per task
+	unsigned long long pos;
+	int task, last, req, next, cur, isum;
+	float bv[4];
+	int bi[4];
+};
+constexpr int kHdrBytes = (int)((sizeof(GroupHdr) + 15) / 16 * 16);
+
+__device__ __forceinline__ long long global_ns()
+{
+	long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+// Next task of a class, or -1 when the worker should stop: every run of the
+// class has retired, the queue stayed empty for kIdleNs, or (error) a
+// reserved slot was never written.
+__device__ int queue_pop(const TickClass& C)
+{
+	volatile QueueCtl* vq = C.ctl;
+	long long idle_since = -1;
+	for (int spins = 0; spins < (1 << 28); spins++) {
+		const unsigned long long h = vq->head, t = vq->tail;
+		if (h < t) {
+			if (atomicCAS(&C.ctl->head, h, h + 1) != h) continue;
+			const unsigned long long want = h / C.cap + 1;
+			volatile unsigned long long* s = C.slots + (h % C.cap);
+			for (int k = 0; k < kSlotSpin; k++) {
+				const unsigned long long v = *s;
+				if ((v >> 32) == want) {
+					__threadfence();
+					return (int)(uint32_t)v;
+				}
+				__nanosleep(64);
+			}
+			atomicExch(&C.ctl->err, 1);
+			return -1;
+		}
+		if (vq->alive <= 0) return -1;
+		const long long now = global_ns();
+		if (idle_since < 0) idle_since = now;
+		else if (now - idle_since > kIdleNs) return -1;
+		__nanosleep(400);
+	}
+	atomicExch(&C.ctl->err, 2);
+	return -1;
+}
+
+// Pushes tasks task_word(w, kind, i), i in [0, n), with the whole group.
+template <int TPP>
+__device__ void queue_push(const TickClass& C, uint32_t w, uint32_t kind, int n, const Group<TPP>& G, GroupHdr& H)
+{
+	if (G.rank == 0) H.pos = atomicAdd(&C.ctl->tail, (unsigned long long)n);
+	G.sync();
+	const unsigned long long p0 = H.pos;
+	__threadfence();
+	for (int i = G.rank; i < n; i += TPP) {
+		const unsigned long long p = p0 + (unsigned long long)i;
+		atomicExch(C.slots + (p % C.cap), ((p / C.cap + 1) << 32) | task_word(w, kind, (uint32_t)i));
+	}
+	G.sync();
+}
+
+template <int TPP>
+__device__ int group_isum(int v, const Group<TPP>& G, GroupHdr& H)
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	if constexpr (TPP == 32) {
+		return v;
+	} else {
+		if (G.rank == 0) H.isum = 0;
+		G.sync();
+		if ((G.rank & 31) == 0) atomicAdd(&H.isum, v);
+		G.sync();
+		const int r = H.isum;
+		G.sync();
+		return r;
+	}
+}
+
+// Lowest energy of a run's population (smallest index on ties) -> best_e, best_g.
+template <int TPP>
+__device__ void best_of_run(const ReqDev& rq, int run, int c, int P, const Group<TPP>& G, GroupHdr& H)
+{
+	const float* E = rq.e[c] + (size_t)run * P;
+	float bv = FLT_MAX;
+	int bi = 0;
+	for (int i = G.rank; i < P; i += TPP)
+		if (E[i] < bv) { bv = E[i]; bi = i; }
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		const float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+		const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+		if (v2 < bv || (v2 == bv && i2 < bi)) { bv = v2; bi = i2; }
+	}
+	if ((G.rank & 31) == 0) { H.bv[G.rank >> 5] = bv; H.bi[G.rank >> 5] = bi; }
+	G.sync();
+	if (G.rank == 0) {
+		for (int w = 1; w < TPP / 32; w++)
+			if (H.bv[w] < H.bv[0] || (H.bv[w] == H.bv[0] && H.bi[w] < H.bi[0])) { H.bv[0] = H.bv[w]; H.bi[0] = H.bi[w]; }
+		rq.best_e[run] = H.bv[0];
+	}
+	G.sync();
+	const float* src = rq.conf[c] + ((size_t)run * P + H.bi[0]) * kGenotypeStride;
+	for (int k = G.rank; k < kGenotypeStride; k += TPP) rq.best_g[(size_t)run * kGenotypeStride + k] = src[k];
+	G.sync();
+}
+
+enum : int { kNextRetire = 0, kNextBest = 1, kNextInit = 2, kNextGA = 3 };
+
 template <int TPP, int LSMET>
-__global__ void __launch_bounds__(kEngineThreads, ADGPU_ENGINE_MIN_CTAS)
-engine_kernel(const ReqDev* __restrict__ reqs, const RunRef* __restrict__ work, uint8_t* work_done, int nwork, int gens_per_tick,
-              unsigned int* counter, int max_atoms, int max_tors)
+__device__ void engine_worker(const TickArgs& t, const TickClass& C)
 {
 	extern __shared__ __align__(16) char smem[];
-	__shared__ KArgs sa;
-	__shared__ int s_item, s_ls, s_done, s_evsum;
-	__shared__ float s_bv[kEngineThreads / 32];
-	__shared__ int s_bi[kEngineThreads / 32];
-	const int gpc = kEngineThreads / TPP, local = threadIdx.x / TPP;
-	const int bytes = group_smem_bytes(max_atoms, max_tors, 64, TPP);
-	GroupSmem S = carve_group(smem + local * bytes, max_atoms, max_tors, 64, TPP);
+	const int local = threadIdx.x / TPP;
+	char* base = smem + (size_t)local * C.group_bytes;
+	GroupHdr& H = *reinterpret_cast<GroupHdr*>(base);
+	char* scratch = base + kHdrBytes;
 	Group<TPP> G;
 	G.rank = threadIdx.x % TPP;
 	G.bar_id = 1 + local;
-	G.red = S.red;
+	G.red = nullptr;
+	if (G.rank == 0) H.req = -1;
+	G.sync();
 	for (;;) {
-		if (threadIdx.x == 0) s_item = (int)atomicAdd(counter, 1u);
-		__syncthreads();
-		const int item = s_item;
-		if (item >= nwork) break;
-		const RunRef rr = work[item];
-		const ReqDev& rq = reqs[rr.req];
+		if (G.rank == 0) H.task = queue_pop(C);
+		G.sync();
+		const int task = H.task;
+		if (task < 0) break;
+		__threadfence();
+		const uint32_t w = (uint32_t)task >> (kTaskIdxBits + 2);
+		const uint32_t kind = ((uint32_t)task >> kTaskIdxBits) & 3u;
+		const int idx = task & (int)((1u << kTaskIdxBits) - 1);
+		const RunRef rr = t.work[w];
+		const ReqDev& rq = t.reqs[rr.req];
 		const int run = rr.run;
-		if (threadIdx.x == 0) sa = rq.a;
-		__syncthreads();
-		// the scratch of a pose group is carved for the class maximum; re-carve
-		// for this ligand's sizes so offsets match what the block functions expect
-		S = carve_group(smem + local * bytes, sa.L.natoms, sa.L.ntors, 64, TPP);
+		if (H.req != rr.req) {
+			const int* src = reinterpret_cast<const int*>(&rq.a);
+			int* dst = reinterpret_cast<int*>(&H.a);
+			for (int i = G.rank; i < (int)(sizeof(KArgs) / 4); i += TPP) dst[i] = src[i];
+			G.sync();
+			if (G.rank == 0) H.req = rr.req;
+		}
+		KArgs& a = H.a;
+		const GroupSmem S = carve_group(scratch, a.L.natoms, a.L.ntors, 64, TPP);
 		G.red = S.red;
-		const int P = sa.dp.pop_size;
-		const uint32_t L = sa.dp.num_of_lsentities;
-		for (int g = 0; g < gens_per_tick; g++) {
-			if (threadIdx.x == 0) {
-				int d = rq.done[run];
-				if (!d && rq.init[run] &&
-				    ((unsigned long long)rq.evals_runs[run] >= rq.max_evals || rq.gen[run] >= rq.max_gens)) {
-					d = 1;
-					rq.done[run] = 1;
-				}
-				s_done = d;
-				s_ls = 0;
-				s_evsum = 0;
-			}
-			__syncthreads();
-			if (s_done) break;
+		const int P = a.dp.pop_size;
+		const int L = (int)a.dp.num_of_lsentities;
+		if (kind != kTaskStart) {
 			const int c = rq.cur[run];
-			if (!rq.init[run]) {
-				// initial population of this run (cuda/kernel1.cu:26-55)
-				if (threadIdx.x == 0) { sa.conf = rq.conf[c]; sa.e = rq.e[c]; }
-				__syncthreads();
-				for (int e = local; e < P; e += gpc) initpop_block<TPP>(sa, (uint32_t)(run * P + e), G, S);
-				__syncthreads();
-				if (threadIdx.x == 0) { rq.init[run] = 1; rq.evals_runs[run] = P; }
-				__syncthreads();
-				continue;
-			}
-			// GA generation (cuda/kernel4.cu): current -> next
-			{
-				if (threadIdx.x == 0) {
-					sa.conf_cur = rq.conf[c]; sa.e_cur = rq.e[c];
-					sa.conf = rq.conf[c ^ 1]; sa.e = rq.e[c ^ 1];
-				}
-				__syncthreads();
-				for (int e = local; e < P; e += gpc) ga_block<TPP>(sa, (uint32_t)(run * P + e), G, S);
-			}
-			__syncthreads();
-			// local search on the next population, entities taken dynamically
-			if (sa.dp.lsearch_rate != 0.0f) {
-				const KArgs& a = sa;          // conf/e already point at the next population
-				for (;;) {
-					uint32_t l = 0;
-					if (G.rank == 0) l = (uint32_t)atomicAdd(&s_ls, 1);
-					if constexpr (TPP == 32) l = __shfl_sync(0xffffffffu, l, 0);
-					else {
-						if (G.rank == 0) S.misc[14] = (int)l;
-						G.sync();
-						l = (uint32_t)S.misc[14];
-						G.sync();
-					}
-					if (l >= L) break;
-					const uint32_t b = (uint32_t)run * L + l;
-					if constexpr (LSMET == LS_SW) sw_block<TPP>(a, b, G, S);
-					else if constexpr (LSMET == LS_AD) gradient_ls_block<TPP, LS_AD>(a, b, G, S);
-					else if constexpr (LSMET == LS_ADAM) gradient_ls_block<TPP, LS_ADAM>(a, b, G, S);
-					else fire_block<TPP>(a, b, G, S);
+			if (G.rank == 0) {
+				if (kind == kTaskInit) { a.conf = rq.conf[c]; a.e = rq.e[c]; a.prng = rq.a.prng; }
+				else if (kind == kTaskGA) {
+					a.conf_cur = rq.conf[c]; a.e_cur = rq.e[c];
+					a.conf = rq.conf[c ^ 1]; a.e = rq.e[c ^ 1];
+					a.prng = rq.a.prng;
+				} else {
+					// local search on the next population; entity l of run r uses
+					// the PRNG states of GA block r*P + l (its own run's range), so
+					// runs in different phases never share states
+					a.conf = rq.conf[c ^ 1]; a.e = rq.e[c ^ 1];
+					a.prng = rq.a.prng + (size_t)run * (size_t)(P - L) * 64;
 				}
 			}
-			__syncthreads();
+			G.sync();
+			if (kind == kTaskLS) {
+				const uint32_t b = (uint32_t)(run * L + idx);
+				if constexpr (LSMET == LS_SW) sw_block<TPP>(a, b, G, S);
+				else if constexpr (LSMET == LS_AD) gradient_ls_block<TPP, LS_AD>(a, b, G, S);
+				else if constexpr (LSMET == LS_ADAM) gradient_ls_block<TPP, LS_ADAM>(a, b, G, S);
+				else fire_block<TPP>(a, b, G, S);
+			} else {
+				const int e0 = idx * t.ga_chunk, e1 = min(P, e0 + t.ga_chunk);
+				for (int e = e0; e < e1; e++) {
+					if (kind == kTaskInit) initpop_block<TPP>(a, (uint32_t)(run * P + e), G, S);
+					else ga_block<TPP>(a, (uint32_t)(run * P + e), G, S);
+				}
+			}
+			// the last task of the phase goes on to finalise it
+			__threadfence();
+			G.sync();
+			if (G.rank == 0) H.last = (atomicSub(&t.pending[w], 1) == 1);
+			G.sync();
+			if (!H.last) continue;
+			__threadfence();
+		}
+		// ---- phase end ----
+		if (kind == kTaskGA && L > 0 && a.dp.lsearch_rate != 0.0f) {
+			if (G.rank == 0) { t.pending[w] = L; __threadfence(); }
+			G.sync();
+			queue_push<TPP>(C, w, kTaskLS, L, G, H);
+			continue;
+		}
+		if (kind == kTaskGA || kind == kTaskLS) {
 			// eval sum of the run (cuda/kernel2.cu:26-52), generation count, buffer flip
-			{
-				int s = 0;
-				for (int i = threadIdx.x; i < P; i += kEngineThreads) s += sa.evals_new[run * P + i];
-				for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-				if ((threadIdx.x & 31) == 0) atomicAdd(&s_evsum, s);
-			}
-			__syncthreads();
-			if (threadIdx.x == 0) {
-				rq.evals_runs[run] += s_evsum;
+			int s = 0;
+			for (int i = G.rank; i < P; i += TPP) s += a.evals_new[run * P + i];
+			s = group_isum<TPP>(s, G, H);
+			if (G.rank == 0) {
+				rq.evals_runs[run] += s;
 				rq.gen[run] += 1;
-				rq.cur[run] = (uint8_t)(c ^ 1);
+				rq.cur[run] = (uint8_t)(rq.cur[run] ^ 1);
+				t.quota[w] -= 1;
 			}
-			__syncthreads();
+		} else if (kind == kTaskInit) {
+			if (G.rank == 0) { rq.init[run] = 1; rq.evals_runs[run] = P; t.quota[w] -= 1; }
 		}
-		// stop test once more, so a run that used its budget in this tick is
-		// reported done now rather than at the start of the next tick
-		__syncthreads();
-		if (threadIdx.x == 0 && !rq.done[run] && rq.init[run] &&
-		    ((unsigned long long)rq.evals_runs[run] >= rq.max_evals || rq.gen[run] >= rq.max_gens))
-			rq.done[run] = 1;
-		__syncthreads();
-		// best member of a finished run's final population
-		if (rq.done[run]) {
-			const int c = rq.cur[run];
-			const float* E = rq.e[c] + (size_t)run * P;
-			float bv = FLT_MAX;
-			int bi = 0;
-			for (int i = threadIdx.x; i < P; i += kEngineThreads)
-				if (E[i] < bv) { bv = E[i]; bi = i; }
-			for (int o = 16; o > 0; o >>= 1) {
-				float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
-				int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-				if (v2 < bv || (v2 == bv && i2 < bi)) { bv = v2; bi = i2; }
-			}
-			if ((threadIdx.x & 31) == 0) { s_bv[threadIdx.x >> 5] = bv; s_bi[threadIdx.x >> 5] = bi; }
-			__syncthreads();
-			if (threadIdx.x == 0) {
-				for (int w = 1; w < kEngineThreads / 32; w++)
-					if (s_bv[w] < s_bv[0] || (s_bv[w] == s_bv[0] && s_bi[w] < s_bi[0])) { s_bv[0] = s_bv[w]; s_bi[0] = s_bi[w]; }
-				rq.best_e[run] = s_bv[0];
-			}
-			__syncthreads();
-			const float* src = rq.conf[c] + ((size_t)run * P + s_bi[0]) * kGenotypeStride;
-			for (int k = threadIdx.x; k < kGenotypeStride; k += kEngineThreads) rq.best_g[(size_t)run * kGenotypeStride + k] = src[k];
+		// stop test (per run: its own evaluations, or its generations)
+		if (G.rank == 0) {
+			int d = rq.done[run], next;
+			if (d) next = kNextRetire;
+			else if (rq.init[run] && ((unsigned long long)rq.evals_runs[run] >= rq.max_evals || rq.gen[run] >= rq.max_gens)) {
+				rq.done[run] = 1;
+				next = kNextBest;
+			} else if (t.quota[w] <= 0) next = kNextRetire;
+			else next = rq.init[run] ? kNextGA : kNextInit;
+			H.next = next;
+			H.cur = rq.cur[run];
 		}
-		if (threadIdx.x == 0) work_done[item] = rq.done[run];
-		__syncthreads();
+		G.sync();
+		const int next = H.next;
+		if (next == kNextGA || next == kNextInit) {
+			const int nch = (P + t.ga_chunk - 1) / t.ga_chunk;
+			if (G.rank == 0) { t.pending[w] = nch; __threadfence(); }
+			G.sync();
+			queue_push<TPP>(C, w, next == kNextGA ? kTaskGA : kTaskInit, nch, G, H);
+			continue;
+		}
+		if (next == kNextBest) best_of_run<TPP>(rq, run, H.cur, P, G, H);
+		if (G.rank == 0) {
+			t.work_done[w] = rq.done[run];
+			__threadfence();
+			atomicSub(&C.ctl->alive, 1);
+		}
+		G.sync();
 	}
+}
+
+// One kernel per local search; its CTAs are split into three ranges, one per
+// threads-per-pose class, each range serving its class's queue.
+template <int LSMET>
+__global__ void __launch_bounds__(kEngineThreads, ADGPU_ENGINE_MIN_CTAS) engine_kernel(const TickArgs t)
+{
+	if ((int)blockIdx.x < t.cls[0].cta_end) engine_worker<32, LSMET>(t, t.cls[0]);
+	else if ((int)blockIdx.x < t.cls[1].cta_end) engine_worker<64, LSMET>(t, t.cls[1]);
+	else engine_worker<128, LSMET>(t, t.cls[2]);
 }
 
 // --------------------------------------------------------------------------
@@ -242,8 +400,15 @@ struct Engine {
 	uint64_t next_id = 1;
 	cudaStream_t stream = nullptr;
 	ReqDev* d_reqs = nullptr; int d_reqs_cap = 0;
+	// per-tick device buffers, grown on demand: work items, their done flags,
+	// phase counters and quotas; the task rings and their control blocks
 	RunRef* d_work = nullptr; int d_work_cap = 0;
-	unsigned int* d_counters = nullptr;
+	uint8_t* d_done = nullptr;
+	int* d_pending = nullptr;
+	int* d_quota = nullptr;
+	unsigned long long* d_slots = nullptr; size_t d_slots_cap = 0;
+	QueueCtl* d_ctl = nullptr;
+	int ga_chunk = 16;
 	std::vector<uint8_t> h_done;
 	std::map<long, int> tpp_cache;     // size bucket -> tuned threads per pose
 	adgpu_engine_stats stats{};
@@ -254,7 +419,8 @@ struct Engine {
 		receptors.clear();
 		if (d_reqs) cudaFree(d_reqs);
 		if (d_work) cudaFree(d_work);
-		if (d_counters) cudaFree(d_counters);
+		if (d_slots) cudaFree(d_slots);
+		if (d_ctl) cudaFree(d_ctl);
 		if (stream) cudaStreamDestroy(stream);
 	}
 };
@@ -266,23 +432,45 @@ static size_t request_bytes(int runs, int pop, size_t tables)
 	       (size_t)runs * (4 + 4 + 3 + 4 + kGenotypeStride * 4) + 1024;
 }
 
-template <int TPP, int LSMET>
-static adgpu_status launch_engine(Engine& E, const RunRef* work, uint8_t* work_done, int nwork, int gens, int max_atoms, int max_tors, unsigned int* counter)
+// Launches the tick's kernel for local search LSMET.  Its CTAs are split
+// between the three threads-per-pose classes in proportion to their work, each
+// class getting no more CTAs than its runs can keep busy at once.
+template <int LSMET>
+static adgpu_status launch_engine(Engine& E, TickArgs t, const int* nruns, const double* weight, const int* max_tasks,
+                                  const int* max_atoms, const int* max_tors)
 {
-	const int bytes = group_smem_bytes(max_atoms, max_tors, 64, TPP) * (kEngineThreads / TPP);
-	auto k = engine_kernel<TPP, LSMET>;
-	if (bytes > 48 * 1024) {
-		cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+	static const int tpps[3] = {32, 64, 128};
+	int smem = 0;
+	for (int k = 0; k < 3; k++) {
+		t.cls[k].group_bytes = kHdrBytes + group_smem_bytes(max_atoms[k], max_tors[k], 64, tpps[k]);
+		if (nruns[k]) smem = std::max(smem, t.cls[k].group_bytes * (kEngineThreads / tpps[k]));
+	}
+	auto kern = engine_kernel<LSMET>;
+	if (smem > 48 * 1024) {
+		cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 		if (e != cudaSuccess) return cuda_fail(e, "engine smem");
 	}
 	int per_sm = 0, dev = 0, sms = 0;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kEngineThreads, bytes);
+	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEngineThreads, smem);
 	if (e != cudaSuccess) return cuda_fail(e, "engine occupancy");
 	if (per_sm < 1) return fail(ADGPU_ERR_LIMIT, "engine kernel does not fit on an SM");
-	int grid = std::min(nwork, per_sm * sms);
-	k<<<grid, kEngineThreads, bytes, E.stream>>>(E.d_reqs, work, work_done, nwork, gens, counter, max_atoms, max_tors);
+	const int total = per_sm * sms;
+	double wsum = 0;
+	for (int k = 0; k < 3; k++) if (nruns[k]) wsum += weight[k];
+	int end = 0;
+	for (int k = 0; k < 3; k++) {
+		int n = 0;
+		if (nruns[k]) {
+			const long useful = ((long)nruns[k] * max_tasks[k] + (kEngineThreads / tpps[k]) - 1) / (kEngineThreads / tpps[k]);
+			n = (int)std::lround(total * (wsum > 0 ? weight[k] / wsum : 1.0));
+			n = (int)std::max<long>(1, std::min<long>(n, useful));
+		}
+		end += n;
+		t.cls[k].cta_end = end;
+	}
+	kern<<<end, kEngineThreads, smem, E.stream>>>(t);
 	e = cudaGetLastError();
 	if (e != cudaSuccess) return cuda_fail(e, "engine launch");
 	return ADGPU_OK;
@@ -318,8 +506,8 @@ adgpu_status adgpu_engine_create(const adgpu_engine_config* cfg, adgpu_engine** 
 	E.budget = E.cfg.memory_budget_bytes ? E.cfg.memory_budget_bytes : (size_t)(0.8 * fr);
 	e = cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking);
 	if (e != cudaSuccess) { delete en; return cuda_fail(e, "stream"); }
-	e = cudaMalloc(&E.d_counters, 64 * sizeof(unsigned int));
-	if (e != cudaSuccess) { delete en; return cuda_fail(e, "engine counters"); }
+	e = cudaMalloc(&E.d_ctl, 12 * sizeof(QueueCtl));
+	if (e != cudaSuccess) { delete en; return cuda_fail(e, "engine queues"); }
 	*out = en;
 	return ADGPU_OK;
 }
@@ -441,83 +629,138 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	if (!en) return fail(ADGPU_ERR_ARG, "null engine");
 	Engine& E = en->e;
 	std::lock_guard<std::mutex> lk(E.mu);
-	// active requests and their runs, grouped by threads-per-pose class
+	// active requests and their runs, grouped by class = threads-per-pose index * 4 + local search
+	constexpr int NC = 12;
 	std::vector<ReqDev> reqs;
 	std::vector<Request*> order;
-	constexpr int NC = 12;                 // classes: threads per pose (3) x local search (4)
 	std::vector<RunRef> work[NC];
-	int max_atoms[NC], max_tors[NC];
-	for (int c = 0; c < NC; c++) { max_atoms[c] = 1; max_tors[c] = 0; }
+	int max_atoms[NC], max_tors[NC], max_tasks[NC];
+	double weight[NC];
+	const int chunk = E.ga_chunk;
+	for (int c = 0; c < NC; c++) { max_atoms[c] = 1; max_tors[c] = 0; max_tasks[c] = 1; weight[c] = 0; }
 	for (auto& kv : E.requests) {
 		Request& r = *kv.second;
 		if (r.done) continue;
-		int cls = (r.tpp == 32 ? 0 : (r.tpp == 64 ? 1 : 2)) * 4 + r.dev.lsmet;
-		int idx = (int)reqs.size();
+		const int cls = (r.tpp == 32 ? 0 : (r.tpp == 64 ? 1 : 2)) * 4 + r.dev.lsmet;
+		const int idx = (int)reqs.size();
 		reqs.push_back(r.dev);
 		order.push_back(&r);
 		for (int k = 0; k < r.runs; k++) work[cls].push_back({idx, k});
+		const adgpu_dockpars& dp = r.dev.a.dp;
 		max_atoms[cls] = std::max(max_atoms[cls], r.natoms);
 		max_tors[cls] = std::max(max_tors[cls], r.ntors);
+		max_tasks[cls] = std::max({max_tasks[cls], (int)dp.num_of_lsentities, (dp.pop_size + chunk - 1) / chunk});
+		weight[cls] += (double)r.runs * (r.dev.a.L.npairs + 8.0 * r.natoms + 64.0);
 	}
 	if (completed) *completed = 0;
 	if (reqs.empty()) return ADGPU_OK;
-	size_t nwork = 0;
-	for (int c = 0; c < NC; c++) nwork += work[c].size();
+	size_t nwork = 0, slots = 0;
+	size_t start[NC], cap[NC], slot0[NC];
+	std::vector<RunRef> all;
+	for (int c = 0; c < NC; c++) {
+		start[c] = all.size();
+		all.insert(all.end(), work[c].begin(), work[c].end());
+		// a run has at most max_tasks tasks queued at once; twice that keeps a
+		// reserved slot from being reused before its previous lap is read
+		cap[c] = work[c].empty() ? 0 : 2 * work[c].size() * (size_t)max_tasks[c] + 1024;
+		slot0[c] = slots;
+		slots += cap[c];
+	}
+	nwork = all.size();
+	if (nwork >= kMaxTickRuns) return fail(ADGPU_ERR_LIMIT, "more than 524287 runs admitted at once");
 	cudaError_t e;
 	if ((int)reqs.size() > E.d_reqs_cap) {
 		if (E.d_reqs) cudaFree(E.d_reqs);
 		E.d_reqs_cap = std::max<int>((int)reqs.size() * 2, 64);
 		e = cudaMalloc(&E.d_reqs, sizeof(ReqDev) * E.d_reqs_cap);
-		if (e != cudaSuccess) return cuda_fail(e, "request table");
+		if (e != cudaSuccess) { E.d_reqs = nullptr; E.d_reqs_cap = 0; return cuda_fail(e, "request table"); }
 	}
 	if ((int)nwork > E.d_work_cap) {
 		if (E.d_work) cudaFree(E.d_work);
 		E.d_work_cap = std::max<int>((int)nwork * 2, 256);
-		e = cudaMalloc(&E.d_work, (sizeof(RunRef) + 1) * E.d_work_cap);
-		if (e != cudaSuccess) return cuda_fail(e, "work list");
+		const size_t per = sizeof(RunRef) + 2 * sizeof(int) + 1;
+		e = cudaMalloc(&E.d_work, per * E.d_work_cap + 256);
+		if (e != cudaSuccess) { E.d_work = nullptr; E.d_work_cap = 0; return cuda_fail(e, "work list"); }
+		char* B = reinterpret_cast<char*>(E.d_work) + sizeof(RunRef) * E.d_work_cap;
+		E.d_pending = reinterpret_cast<int*>(B);
+		E.d_quota = E.d_pending + E.d_work_cap;
+		E.d_done = reinterpret_cast<uint8_t*>(E.d_quota + E.d_work_cap);
 	}
-	std::vector<RunRef> all;
-	all.reserve(nwork);
-	size_t start[NC];
-	for (int c = 0; c < NC; c++) { start[c] = all.size(); all.insert(all.end(), work[c].begin(), work[c].end()); }
-	uint8_t* d_done = reinterpret_cast<uint8_t*>(E.d_work + E.d_work_cap);
+	if (slots > E.d_slots_cap) {
+		if (E.d_slots) cudaFree(E.d_slots);
+		E.d_slots_cap = slots * 2;
+		e = cudaMalloc(&E.d_slots, E.d_slots_cap * sizeof(unsigned long long));
+		if (e != cudaSuccess) { E.d_slots = nullptr; E.d_slots_cap = 0; return cuda_fail(e, "task rings"); }
+	}
+	// initial state: every run's START task queued in its class's ring (lap 1),
+	// the rest of the ring empty (lap 0 matches no position)
+	std::vector<unsigned long long> h_start(nwork);
+	std::vector<int> h_quota(nwork, E.cfg.gens_per_tick);
+	QueueCtl h_ctl[NC];
+	memset(h_ctl, 0, sizeof(h_ctl));
+	for (int c = 0; c < NC; c++) {
+		for (size_t i = 0; i < work[c].size(); i++)
+			h_start[start[c] + i] = (1ull << 32) | task_word((uint32_t)(start[c] + i), kTaskStart, 0);
+		h_ctl[c].tail = work[c].size();
+		h_ctl[c].alive = (int)work[c].size();
+	}
 	e = cudaMemcpyAsync(E.d_reqs, reqs.data(), sizeof(ReqDev) * reqs.size(), cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_work, all.data(), sizeof(RunRef) * nwork, cudaMemcpyHostToDevice, E.stream);
-	if (e == cudaSuccess) e = cudaMemsetAsync(E.d_counters, 0, NC * sizeof(unsigned int), E.stream);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_quota, h_quota.data(), sizeof(int) * nwork, cudaMemcpyHostToDevice, E.stream);
+	if (e == cudaSuccess) e = cudaMemsetAsync(E.d_done, 0, nwork, E.stream);
+	if (e == cudaSuccess) e = cudaMemsetAsync(E.d_slots, 0, slots * sizeof(unsigned long long), E.stream);
+	for (int c = 0; c < NC && e == cudaSuccess; c++)
+		if (!work[c].empty())
+			e = cudaMemcpyAsync(E.d_slots + slot0[c], h_start.data() + start[c], work[c].size() * sizeof(unsigned long long),
+			                    cudaMemcpyHostToDevice, E.stream);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_ctl, h_ctl, sizeof(h_ctl), cudaMemcpyHostToDevice, E.stream);
 	if (e != cudaSuccess) return cuda_fail(e, "tick upload");
-	const int gens = E.cfg.gens_per_tick;
-	for (int c = 0; c < NC; c++) {
-		if (work[c].empty()) continue;
-		adgpu_status st = ADGPU_OK;
-		const RunRef* w = E.d_work + start[c];
-		uint8_t* wd = d_done + start[c];
-		int n = (int)work[c].size();
-		unsigned int* ctr = E.d_counters + c;
-#define ADGPU_ENGINE_CASE(ID, TPP, LS) \
-		case ID: st = launch_engine<TPP, LS>(E, w, wd, n, gens, max_atoms[c], max_tors[c], ctr); break;
-		switch (c) {
-			ADGPU_ENGINE_CASE(0, 32, LS_SW) ADGPU_ENGINE_CASE(1, 32, LS_AD) ADGPU_ENGINE_CASE(2, 32, LS_ADAM) ADGPU_ENGINE_CASE(3, 32, LS_FIRE)
-			ADGPU_ENGINE_CASE(4, 64, LS_SW) ADGPU_ENGINE_CASE(5, 64, LS_AD) ADGPU_ENGINE_CASE(6, 64, LS_ADAM) ADGPU_ENGINE_CASE(7, 64, LS_FIRE)
-			ADGPU_ENGINE_CASE(8, 128, LS_SW) ADGPU_ENGINE_CASE(9, 128, LS_AD) ADGPU_ENGINE_CASE(10, 128, LS_ADAM) ADGPU_ENGINE_CASE(11, 128, LS_FIRE)
+	for (int m = 0; m < 4; m++) {
+		int nr[3], ma[3], mt[3], mx[3];
+		double wt[3];
+		bool any = false;
+		TickArgs t;
+		memset(&t, 0, sizeof(t));
+		t.reqs = E.d_reqs; t.work = E.d_work; t.work_done = E.d_done;
+		t.pending = E.d_pending; t.quota = E.d_quota; t.ga_chunk = chunk;
+		for (int k = 0; k < 3; k++) {
+			const int c = k * 4 + m;
+			nr[k] = (int)work[c].size(); ma[k] = max_atoms[c]; mt[k] = max_tors[c]; mx[k] = max_tasks[c]; wt[k] = weight[c];
+			t.cls[k].slots = E.d_slots + slot0[c];
+			t.cls[k].ctl = E.d_ctl + c;
+			t.cls[k].cap = (uint32_t)cap[c];
+			any |= nr[k] > 0;
 		}
-#undef ADGPU_ENGINE_CASE
+		if (!any) continue;
+		adgpu_status st = ADGPU_OK;
+		switch (m) {
+		case LS_SW: st = launch_engine<LS_SW>(E, t, nr, wt, mx, ma, mt); break;
+		case LS_AD: st = launch_engine<LS_AD>(E, t, nr, wt, mx, ma, mt); break;
+		case LS_ADAM: st = launch_engine<LS_ADAM>(E, t, nr, wt, mx, ma, mt); break;
+		default: st = launch_engine<LS_FIRE>(E, t, nr, wt, mx, ma, mt); break;
+		}
 		if (st != ADGPU_OK) return st;
 	}
 	E.h_done.resize(nwork);
-	e = cudaMemcpyAsync(E.h_done.data(), d_done, nwork, cudaMemcpyDeviceToHost, E.stream);
+	e = cudaMemcpyAsync(E.h_done.data(), E.d_done, nwork, cudaMemcpyDeviceToHost, E.stream);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(h_ctl, E.d_ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, E.stream);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
 	if (e != cudaSuccess) return cuda_fail(e, "engine tick");
+	for (int c = 0; c < NC; c++) {
+		if (h_ctl[c].err) return fail(ADGPU_ERR_TIMEOUT, "engine task queue: a reserved slot was never written");
+		if (h_ctl[c].alive != 0) return fail(ADGPU_ERR_STATE, "engine tick ended with runs still active");
+	}
 	E.stats.ticks++;
 	// a request is complete when all its runs are
 	std::vector<int> runs_done(order.size(), 0);
 	for (size_t i = 0; i < nwork; i++)
 		if (E.h_done[i]) runs_done[all[i].req]++;
 	int comp = 0;
-	double t = now_s();
+	double tnow = now_s();
 	for (size_t i = 0; i < order.size(); i++)
 		if (runs_done[i] == order[i]->runs) {
 			order[i]->done = true;
-			order[i]->t_done = t;
+			order[i]->t_done = tnow;
 			comp++;
 		}
 	E.stats.completed += comp;

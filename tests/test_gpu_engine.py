@@ -26,17 +26,20 @@ def ligand(grid, idx, n_heavy, n_tors, runs=4, pop=150):
 
 @pytest.mark.parametrize("lsmet", ["ad", "sw"])
 def test_engine_matches_plain_path(grid, lsmet):
-    """With a generation budget both paths stop at the same generation, so every
-    run must come out identical (same kernels, same PRNG states)."""
-    lig = ligand(grid, 0, 16, 4, runs=3)
+    """With a generation budget both paths stop at the same generation, so the
+    run must come out identical (same kernels, same PRNG states).  One run:
+    the engine gives local-search entity l of run r the PRNG states of GA
+    block r*P + l (so that runs in different phases never share states), which
+    for run 0 are the reference's own (block l)."""
+    lig = ligand(grid, 0, 16, 4, runs=1)
     gens = 6
     # plain: reference kernel API, resident loop
-    job = device.DeviceJob(lig.tables, lig.dockpars, grid.reference_layout(), 3, lig.prng)
+    job = device.DeviceJob(lig.tables, lig.dockpars, grid.reference_layout(), 1, lig.prng)
     job.activate()
     res = dock.dock(job, lig.initpop, lsmet, nev=10**9, ngen=gens)
     assert res.generations == gens
     P = lig.dockpars.pop_size
-    e_plain = res.energies.cpu().numpy().reshape(3, P)
+    e_plain = res.energies.cpu().numpy().reshape(1, P)
     # engine
     en = engine.Engine(threads_per_pose=32)
     rec = en.add_receptor(grid)
