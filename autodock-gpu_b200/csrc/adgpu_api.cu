@@ -161,9 +161,28 @@ adgpu_status launch_lga(const KArgs& a, float* grads, cudaStream_t stream, int c
 	return ADGPU_OK;
 }
 
+// Threads per pose for a launch of n blocks when none is configured: the
+// largest group size (128, then 64) that still leaves every block a pose
+// group with all of them resident at once (6 CTAs of 128 threads per SM).
+// A per-ligand launch of a few runs has few local-search entities, and more
+// threads per pose then shorten each entity's chain of evaluations.
+static int auto_tpp(uint32_t n)
+{
+	if (g_num_sms == 0) {
+		int dev = 0;
+		if (cudaGetDevice(&dev) != cudaSuccess ||
+		    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 32;
+	}
+	const long groups32 = (long)g_num_sms * ADGPU_MIN_CTAS * 4;
+	if ((long)n * 4 <= groups32) return 128;
+	if ((long)n * 2 <= groups32) return 64;
+	return 32;
+}
+
 template <int KIND>
 adgpu_status launch_kind(const KArgs& a, float* grads, cudaStream_t stream, int tpp)
 {
+	if (tpp == 0) tpp = auto_tpp(a.nblocks);
 	switch (tpp) {
 	case 32: return launch_lga<32, KIND>(a, grads, stream, 128);
 	case 64: return launch_lga<64, KIND>(a, grads, stream, 128);
@@ -180,7 +199,7 @@ struct ApiState {
 	bool ready = false;
 	adgpu_gpudata data;
 	LigandTables tables;       // host-repacked + device copy
-	int tpp = 32;
+	int tpp = 0;               // threads per pose; 0: chosen per launch (auto_tpp)
 	unsigned int* counters = nullptr;   // library-owned work counters of the local-search launches
 	std::mutex mu;
 };
@@ -306,6 +325,7 @@ adgpu_status adgpu_set_kernels_gpu_data(const adgpu_gpudata* data)
 	s.data = *data;
 	adgpu_status st = build_ligand_tables_from_device(*data, s.tables);
 	if (st != ADGPU_OK) return st;
+	s.tpp = 0;
 	if (const char* t = getenv("ADGPU_THREADS_PER_POSE")) s.tpp = atoi(t);
 	if (!s.counters) ADGPU_CUDA(cudaMalloc(&s.counters, 16 * sizeof(unsigned int)), "work counters");
 	s.ready = true;

@@ -49,6 +49,22 @@ struct __align__(16) PairRec {
 	uint32_t pad;
 };
 
+// Stored position of element p of a list of n (pairs, torsion items) in
+// warp-interleaved order.  The reference lists pairs by first atom and items
+// by torsion, so 32 consecutive entries mostly share an atom or a torsion and
+// a warp's shared-memory gradient atomics on it would serialise.  The list is
+// cut into up to 32 consecutive stretches of K entries and stored row by row:
+// one warp instruction reads one entry of each stretch.  Sums over the list
+// are fixed-point (order-free) or float energies (order within rounding).
+__host__ __device__ inline uint32_t interleave_pos(uint32_t p, uint32_t n)
+{
+	const uint32_t K = (n + 31) / 32;                    // stretch length
+	if (K <= 1) return p;
+	const uint32_t full = n / K, rem = n - full * K;     // full stretches; length of the last, partial one
+	const uint32_t l = p / K, k = p % K;                 // stretch, row
+	return k * full + (k < rem ? k : rem) + l;
+}
+
 struct LigDev {
 	// sizes
 	int natoms, nlig, ngenes, ntors, npairs, ntoritems;

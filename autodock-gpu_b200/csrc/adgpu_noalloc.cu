@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256) noalloc_repack_kernel(adgpu_gpudata d, Li
 		for (int c = 0; c < s_istart[k + 1] - s_istart[k]; c++) {
 			int la = d.pMem_rotbonds_atoms_const[ADGPU_MAX_ATOMS * k + c];
 			if (la < 0 || la >= N) { status[0] = 1; la = 0; }
-			items[s_istart[k] + c] = ((uint32_t)k << 8) | (uint32_t)la;
+			items[interleave_pos((uint32_t)(s_istart[k] + c), (uint32_t)s_istart[NT])] = ((uint32_t)k << 8) | (uint32_t)la;
 		}
 	}
 	// intramolecular pairs
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(256) noalloc_repack_kernel(adgpu_gpudata d, Li
 		r.vbond = cgg0 ? 50.0f : 0.0f;
 		r.ij = a1 | (a2 << 8) | (m << 16) | (n << 24);
 		r.pad = 0;
-		pr[p] = r;
+		pr[interleave_pos((uint32_t)p, (uint32_t)Q)] = r;
 	}
 	__syncthreads();
 	if (threadIdx.x == 0) {

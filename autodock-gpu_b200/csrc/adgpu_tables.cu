@@ -119,7 +119,9 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 		mv[k] = make_float4(cf.rotbonds_moving_vectors_const[3 * k], cf.rotbonds_moving_vectors_const[3 * k + 1], cf.rotbonds_moving_vectors_const[3 * k + 2], 0.f);
 		ends[k] = make_int2(rotbonds[2 * k], rotbonds[2 * k + 1]);
 	}
-	memcpy(B + out.off_tor_items, items.data(), items.size() * 4);
+	// pairs and torsion items in warp-interleaved order (interleave_pos)
+	uint32_t* it_out = reinterpret_cast<uint32_t*>(B + out.off_tor_items);
+	for (size_t i = 0; i < items.size(); i++) it_out[interleave_pos((uint32_t)i, (uint32_t)items.size())] = items[i];
 	PairRec* pr = reinterpret_cast<PairRec*>(B + out.off_pairs);
 	const int nat = dp.num_of_atypes;
 	for (int p = 0; p < Q; p++) {
@@ -143,7 +145,7 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 		r.vbond = cgg0 ? 50.0f : 0.0f;
 		r.ij = a1 | (a2 << 8) | (m << 16) | (n << 24);
 		r.pad = 0;
-		pr[p] = r;
+		pr[interleave_pos((uint32_t)p, (uint32_t)Q)] = r;
 	}
 	return ADGPU_OK;
 }

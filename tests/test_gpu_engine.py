@@ -25,7 +25,7 @@ def ligand(grid, idx, n_heavy, n_tors, runs=4, pop=150):
 
 
 @pytest.mark.parametrize("lsmet", ["ad", "sw"])
-def test_engine_matches_plain_path(grid, lsmet):
+def test_engine_matches_plain_path(grid, lsmet, monkeypatch):
     """With a generation budget both paths stop at the same generation, so the
     run must come out identical (same kernels, same PRNG states).  One run:
     the engine gives local-search entity l of run r the PRNG states of GA
@@ -33,7 +33,8 @@ def test_engine_matches_plain_path(grid, lsmet):
     for run 0 are the reference's own (block l)."""
     lig = ligand(grid, 0, 16, 4, runs=1)
     gens = 6
-    # plain: reference kernel API, resident loop
+    # plain: reference kernel API, resident loop, with the engine's group size
+    monkeypatch.setenv("ADGPU_THREADS_PER_POSE", "32")
     job = device.DeviceJob(lig.tables, lig.dockpars, grid.reference_layout(), 1, lig.prng)
     job.activate()
     res = dock.dock(job, lig.initpop, lsmet, nev=10**9, ngen=gens)
