@@ -143,9 +143,13 @@ adgpu_status launch_lga(const KArgs& a, float* grads, cudaStream_t stream, int c
 	const int gpc = cta_threads / TPP;
 	const int bytes = group_smem_bytes(a.L.natoms, a.L.ntors, (int)a.ref_threads, TPP) * gpc;
 	auto kfn = lga_kernel<TPP, KIND>;
-	static thread_local int configured_bytes[2] = {-1, -1};
-	(void)configured_bytes;
 	if (bytes > 48 * 1024) ADGPU_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "smem attribute");
+	static int carveout = -2;           // per instantiation: the last preference set
+	const int pct = smem_carveout_pct(bytes, ADGPU_MIN_CTAS);
+	if (pct >= 0 && pct > carveout) {
+		ADGPU_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, pct), "carveout");
+		carveout = pct;
+	}
 	int per_sm = 0;
 	ADGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, cta_threads, bytes), "occupancy");
 	if (per_sm < 1) return fail(ADGPU_ERR_LIMIT, "kernel does not fit on an SM");
@@ -161,11 +165,12 @@ adgpu_status launch_lga(const KArgs& a, float* grads, cudaStream_t stream, int c
 	return ADGPU_OK;
 }
 
-// Threads per pose for a launch of n blocks when none is configured: the
-// largest group size (128, then 64) that still leaves every block a pose
-// group with all of them resident at once (6 CTAs of 128 threads per SM).
-// A per-ligand launch of a few runs has few local-search entities, and more
-// threads per pose then shorten each entity's chain of evaluations.
+// Threads per pose for a launch of n blocks when none is configured: 64 when
+// every block still gets a resident pose group of 64 threads (6 CTAs of 128
+// threads per SM), else 32.  A per-ligand launch of a few runs has few
+// local-search entities, and two warps per pose then shorten each entity's
+// chain of evaluations; on B200, 64 beat both 32 and 128 for per-ligand
+// dockings of 20 and of 100 runs (10-64 heavy atoms).
 static int auto_tpp(uint32_t n)
 {
 	if (g_num_sms == 0) {
@@ -174,9 +179,7 @@ static int auto_tpp(uint32_t n)
 		    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 32;
 	}
 	const long groups32 = (long)g_num_sms * ADGPU_MIN_CTAS * 4;
-	if ((long)n * 4 <= groups32) return 128;
-	if ((long)n * 2 <= groups32) return 64;
-	return 32;
+	return (long)n * 2 <= groups32 ? 64 : 32;
 }
 
 template <int KIND>

@@ -150,10 +150,17 @@ struct Group {
 	int bar_id;        // named barrier for TPP > 32
 	float* red;        // TPP/32 * 8 floats of scratch for cross-warp reductions
 
+	// Barrier ids are immediates so that a kernel reserves only the ids it
+	// uses (a register id makes ptxas reserve all 16, which caps resident
+	// CTAs per SM at 4).  A 128-thread group is a whole 128-thread CTA.
 	__device__ __forceinline__ void sync() const
 	{
 		if constexpr (TPP == 32) __syncwarp();
-		else asm volatile("bar.sync %0, %1;" :: "r"(bar_id), "r"(TPP) : "memory");
+		else if constexpr (TPP == 128) __syncthreads();
+		else {
+			if (bar_id == 1) asm volatile("bar.sync 1, 64;" ::: "memory");
+			else asm volatile("bar.sync 2, 64;" ::: "memory");
+		}
 	}
 
 	__device__ __forceinline__ float sum(float v) const

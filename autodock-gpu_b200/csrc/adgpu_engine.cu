@@ -450,6 +450,11 @@ static adgpu_status launch_engine(Engine& E, TickArgs t, const int* nruns, const
 		cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 		if (e != cudaSuccess) return cuda_fail(e, "engine smem");
 	}
+	const int pct = smem_carveout_pct(smem, ADGPU_ENGINE_MIN_CTAS);
+	if (pct >= 0) {
+		cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+		if (e != cudaSuccess) return cuda_fail(e, "engine carveout");
+	}
 	int per_sm = 0, dev = 0, sms = 0;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -848,8 +853,12 @@ adgpu_status adgpu_engine_request_info(adgpu_engine* en, uint64_t request_id, in
 
 namespace adgpu {
 
-// Scores a fixed set of poses of the request's ligand with each group size and
-// keeps the fastest; cached per (atoms/16, pairs/256) bucket.
+// Scores the request's poses with each group size and keeps the fastest;
+// cached per (atoms/16, pairs/256) bucket.  Every pose is scored kTuneReps
+// times by a grid that fills the GPU, so the timing is the steady-state
+// throughput the engine sees, not the tail of one pass over a few thousand
+// poses (repeated scorings of a pose write the same values).
+constexpr uint32_t kTuneReps = 8;
 template <int TPP>
 __global__ void __launch_bounds__(128) tune_kernel(KArgs a, float* grads)
 {
@@ -857,7 +866,7 @@ __global__ void __launch_bounds__(128) tune_kernel(KArgs a, float* grads)
 	Group<TPP> G;
 	GroupSmem S;
 	group_of<TPP>(a, gid, ngroups, G, S);
-	for (uint32_t b = gid; b < a.nblocks; b += ngroups) score_block<TPP, true>(a, b, G, S, grads);
+	for (uint32_t i = gid; i < kTuneReps * a.nblocks; i += ngroups) score_block<TPP, true>(a, i % a.nblocks, G, S, grads);
 }
 
 template <int TPP>
@@ -872,7 +881,7 @@ static float time_tpp(Engine& E, const KArgs& a, float* grads)
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, bytes);
 	if (per_sm < 1) return 1e30f;
-	int grid = std::min<int>((int)((a.nblocks + gpc - 1) / gpc), per_sm * sms);
+	int grid = std::min<int>((int)((kTuneReps * a.nblocks + gpc - 1) / gpc), per_sm * sms);
 	cudaEvent_t t0, t1;
 	cudaEventCreate(&t0);
 	cudaEventCreate(&t1);

@@ -43,6 +43,21 @@ struct GroupSmem {
 	float* miscf;     // small floats (random numbers, energies)
 };
 
+// Shared-memory carveout (percent of the SM's maximum) that lets `ctas` CTAs
+// of `bytes` dynamic shared memory each be resident at once; the rest of the
+// unified L1/shared array stays L1 cache for the ligand tables and the maps.
+// (With no preference the driver picked a 100 KB split: 4 engine CTAs per SM.)
+inline int smem_carveout_pct(int bytes, int ctas)
+{
+	int dev = 0, max_sm = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess ||
+	    cudaDeviceGetAttribute(&max_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess || max_sm <= 0)
+		return -1;
+	const long need = (long)ctas * (bytes + 1024);
+	const long pct = (need * 100 + max_sm - 1) / max_sm;
+	return (int)(pct > 100 ? 100 : pct);
+}
+
 __host__ __device__ inline int group_smem_bytes(int natoms, int ntors, int ref_threads, int tpp)
 {
 	int b = pose_smem_bytes(natoms, ntors);

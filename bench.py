@@ -386,7 +386,7 @@ def _ligand_text(config_id, idx, n_heavy, n_tors, types=None):
 
 def run_batch(args):
     """--mode batch: uneven ligands docked by the batch engine (all ligands and
-    runs in one persistent launch per threads-per-pose class) next to plain
+    runs admitted at once, one persistent launch) next to plain
     per-ligand dockings through the reference kernel API, same ligands, same
     budget.  A bounded sample of the batching configuration (1024 ligands,
     10-64 heavy atoms, 0-32 torsions, nrun 20, 2.5M evals per run)."""
@@ -402,16 +402,19 @@ def run_batch(args):
     ligs = [frontend.Ligand(grid, _ligand_text(3, i, a, t), None, run=run, seed=w["seed"], num_runs=nrun)
             for i, (a, t) in enumerate(sizes)]
     # batched: one engine, everything admitted, run to completion
-    en = engine.Engine(threads_per_pose=args.tpp if args.tpp != 32 else 0)
+    en = engine.Engine(threads_per_pose=args.engine_tpp)
     rec = en.add_receptor(grid)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ids = [en.submit(lg, rec, args.lsmet, max_evals=nev) for lg in ligs]
+    tpps = {}
+    for i in ids:
+        t = en.info(i)[0]
+        tpps[str(t)] = tpps.get(str(t), 0) + 1
     en.run()
     res = [en.result(i) for i in ids]
     t_batch = time.perf_counter() - t0
     ev_batch = sum(int(r.evals.sum()) for r in res)
-    tpps = {}
     # plain: one ligand at a time through the kernel API, (a) driven by the
     # reference host's loop (a synchronous call per kernel per generation) --
     # the drop-in -- and (b) with the loop resident on the device
@@ -526,6 +529,8 @@ def main():
     ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel", "batch", "serve"])
     ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel mode)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
+    ap.add_argument("--engine-tpp", type=int, default=0,
+                    help="engine threads per pose (batch mode): 0 = autotuned per ligand size, or 32, 64, 128")
     ap.add_argument("--nlig", type=int, default=64, help="ligands (batch mode)")
     ap.add_argument("--nev", type=int, default=250_000, help="evaluations per run (batch / serve modes)")
     ap.add_argument("--plain-sample", type=int, default=16, help="ligands docked one at a time for the plain arm")
