@@ -132,6 +132,12 @@ __device__ __forceinline__ int quant(float v)
 	return __float2int_rn(fminf(kMaxTerm, fmaxf(-kMaxTerm, kTermScale * v)));
 }
 
+// quant() of v / kTermScale: for a value already multiplied by the scale.
+__device__ __forceinline__ int quant_scaled(float v)
+{
+	return __float2int_rn(fminf(kMaxTerm, fmaxf(-kMaxTerm, v)));
+}
+
 // ---- PRNG: the reference's per-thread LCG (cuda/auxiliary_genetic.cu:29-79) ------
 __device__ __forceinline__ uint32_t lcg_next(uint32_t& s) { s = 1103515245u * s + 12345u; return s; }
 __device__ __forceinline__ float lcg_float(uint32_t& s) { return ((float)lcg_next(s) / 4294967296.0f) * 0.999999f; }
@@ -205,10 +211,12 @@ struct Group {
 };
 
 // ---- per-pose shared-memory scratch -------------------------------------------------
-// Layout (floats/ints, natoms rounded up to a multiple of 4):
-//   x, y, z [N]; fx, fy, fz [N] (int); tq [ntors] float4; gg [64] int
+// Layout (natoms rounded up to a multiple of 4):
+//   tq [ntors] float4; xyz [N] float4 (x, y, z, 0); fx, fy, fz [N] int; gg [64] int
+// An atom's coordinates are one 16-byte load, so a pair reads both its atoms
+// with two shared-memory loads.
 struct PoseSmem {
-	float* x; float* y; float* z;
+	float4* xyz;
 	int* fx; int* fy; int* fz;
 	float4* tq;
 	int* gg;
@@ -217,7 +225,7 @@ struct PoseSmem {
 __host__ __device__ inline int pose_smem_bytes(int natoms, int ntors)
 {
 	int n4 = (natoms + 3) & ~3;
-	return (6 * n4) * 4 + ntors * 16 + 64 * 4;
+	return (7 * n4) * 4 + ntors * 16 + 64 * 4;
 }
 
 __device__ __forceinline__ PoseSmem carve_pose(char* base, int natoms, int ntors)
@@ -227,8 +235,9 @@ __device__ __forceinline__ PoseSmem carve_pose(char* base, int natoms, int ntors
 	float* f = reinterpret_cast<float*>(base);
 	s.tq = reinterpret_cast<float4*>(f);          // 16-byte aligned first
 	f += ntors * 4;
-	s.x = f; s.y = f + n4; s.z = f + 2 * n4;
-	s.fx = reinterpret_cast<int*>(f + 3 * n4);
+	s.xyz = reinterpret_cast<float4*>(f);         // still 16-byte aligned
+	f += 4 * n4;
+	s.fx = reinterpret_cast<int*>(f);
 	s.fy = s.fx + n4; s.fz = s.fy + n4;
 	s.gg = s.fz + n4;
 	return s;
@@ -286,7 +295,9 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	G.sync();
 
 	// 2. pose: each atom applies its own torsion chain, then the general rotation
-	//    (the per-atom order the reference's rotation list encodes, cuda/calcMergeEneGra.cu:131-190)
+	//    (the per-atom order the reference's rotation list encodes, cuda/calcMergeEneGra.cu:131-190);
+	//    the same thread then takes the atom's intermolecular terms (3.)
+	float e_acc = 0.0f;
 	for (int a = rank; a < L.natoms; a += TPP) {
 		float4 r4 = L.atom_xyzq[a];
 		float3 p = make_float3(r4.x, r4.y, r4.z);
@@ -304,19 +315,14 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 			p = qrot(p, gr.q);
 			p.x += gr.mv.x; p.y += gr.mv.y; p.z += gr.mv.z;
 		}
-		S.x[a] = p.x; S.y[a] = p.y; S.z[a] = p.z;
-	}
-	G.sync();
+		S.xyz[a] = make_float4(p.x, p.y, p.z, 0.0f);
 
-	// 3. intermolecular: trilinear interpolation of the type, e and d maps
-	//    (cuda/calcMergeEneGra.cu:195-413)
-	float e_acc = 0.0f;
-	for (int a = rank; a < L.natoms; a += TPP) {
-		uint32_t info = L.atom_info[a];
+		// 3. intermolecular: trilinear interpolation of the type, e and d maps
+		//    (cuda/calcMergeEneGra.cu:195-413)
 		int fx = 0, fy = 0, fz = 0;
 		if (!(info & 0x100u)) {
-			float x = S.x[a], y = S.y[a], z = S.z[a];
-			float q = L.atom_xyzq[a].w;
+			float x = p.x, y = p.y, z = p.z;
+			float q = r4.w;
 			if (x < 0.f || y < 0.f || z < 0.f || x >= (float)(L.gx - 1) || y >= (float)(L.gy - 1) || z >= (float)(L.gz - 1)) {
 				e_acc += kOutOfGridPenalty;
 				fx = fy = fz = kOutOfGridForce;
@@ -368,7 +374,7 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 		}
 		if (GRAD) { S.fx[a] = fx; S.fy[a] = fy; S.fz[a] = fz; }
 	}
-	if (GRAD) G.sync();
+	G.sync();
 
 	// 4. intramolecular pairs (cuda/calcMergeEneGra.cu:418-602)
 	// The reference's terms, rewritten with one reciprocal square root and two
@@ -379,7 +385,8 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 		float4 A = __ldg(pr), B = __ldg(pr + 1);
 		uint32_t ij = __float_as_uint(B.z);
 		int a1 = ij & 0xFF, a2 = (ij >> 8) & 0xFF;
-		float subx = S.x[a1] - S.x[a2], suby = S.y[a1] - S.y[a2], subz = S.z[a1] - S.z[a2];
+		const float4 p1 = S.xyz[a1], p2 = S.xyz[a2];
+		float subx = p1.x - p2.x, suby = p1.y - p2.y, subz = p1.z - p2.z;
 		float d2g = subx * subx + suby * suby + subz * subz;
 		float inv_dist = rsqrtf(d2g);
 		float dist = d2g > 0.0f ? d2g * inv_dist : 0.0f;
@@ -422,8 +429,10 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 			if (GRAD) pg += -(es * inv_r) * diel - es * 2.21718f * rs2 * rs - 0.0771605f * r * desolv;
 		}
 		if (GRAD) {
-			float gdd = -pg * inv_dist;
-			int ix = quant(subx * gdd), iy = quant(suby * gdd), iz = quant(subz * gdd);
+			// quant(sub * gdd) with the 1024 scale folded into gdd (a power of
+			// two: the same rounding, one multiply instead of three)
+			const float gdd = -pg * inv_dist * kTermScale;
+			const int ix = quant_scaled(subx * gdd), iy = quant_scaled(suby * gdd), iz = quant_scaled(subz * gdd);
 			atomicSub(&S.fx[a1], ix); atomicSub(&S.fy[a1], iy); atomicSub(&S.fz[a1], iz);
 			atomicAdd(&S.fx[a2], ix); atomicAdd(&S.fy[a2], iy); atomicAdd(&S.fz[a2], iz);
 		}
@@ -435,7 +444,8 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	// 5. torque and total force over the ligand atoms (cuda/calcMergeEneGra.cu:608-661)
 	float red[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 	for (int a = rank; a < L.nlig; a += TPP) {
-		float3 r = make_float3((S.x[a] - gr.mv.x) * L.spacing, (S.y[a] - gr.mv.y) * L.spacing, (S.z[a] - gr.mv.z) * L.spacing);
+		const float4 pa = S.xyz[a];
+		float3 r = make_float3((pa.x - gr.mv.x) * L.spacing, (pa.y - gr.mv.y) * L.spacing, (pa.z - gr.mv.z) * L.spacing);
 		float3 f = make_float3(kOneOverTermScale * (float)S.fx[a], kOneOverTermScale * (float)S.fy[a], kOneOverTermScale * (float)S.fz[a]);
 		red[3] += f.x; red[4] += f.y; red[5] += f.z;
 		float3 t = cross3(r, f);
@@ -476,11 +486,12 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 		uint32_t item = L.tor_items[it];
 		int k = item >> 8, la = item & 0xFF;
 		int2 ends = L.tors_ends[k];
-		float rx = S.x[ends.x], ry = S.y[ends.x], rz = S.z[ends.x];
-		float ux = S.x[ends.y] - rx, uy = S.y[ends.y] - ry, uz = S.z[ends.y] - rz;
+		const float4 e0 = S.xyz[ends.x], e1 = S.xyz[ends.y], pl = S.xyz[la];
+		float rx = e0.x, ry = e0.y, rz = e0.z;
+		float ux = e1.x - rx, uy = e1.y - ry, uz = e1.z - rz;
 		float l = rnorm3df(ux, uy, uz);
 		ux *= l; uy *= l; uz *= l;
-		float3 r = make_float3(S.x[la] - rx, S.y[la] - ry, S.z[la] - rz);
+		float3 r = make_float3(pl.x - rx, pl.y - ry, pl.z - rz);
 		float3 f = make_float3(kOneOverTermScale * (float)S.fx[la], kOneOverTermScale * (float)S.fy[la], kOneOverTermScale * (float)S.fz[la]);
 		float3 t = cross3(r, f);
 		float on_axis = (ux * t.x + uy * t.y + uz * t.z) * L.spacing;

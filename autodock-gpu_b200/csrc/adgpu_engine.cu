@@ -87,7 +87,11 @@ struct QueueCtl {
 	unsigned long long tail;    // next position to push
 	int alive;                  // runs of the class not yet retired in this tick
 	int err;                    // nonzero: a reserved slot was never written
-	int pad[2];
+	int workers;                // pose groups that served this class
+	int pad;
+	// accounting (globaltimer ns): time pose groups spent on tasks, tasks done,
+	// first worker start and last worker exit
+	unsigned long long busy_ns, tasks, t_first, t_last;
 };
 
 struct TickClass {
@@ -112,6 +116,8 @@ struct TickArgs {
 struct GroupHdr {
 	KArgs a;                    // the current request's arguments, pointers set per task
 	unsigned long long pos;
+	long long t_enter, t_task;           // worker accounting (rank 0 only)
+	unsigned long long busy, ntask;
 	int task, last, req, next, cur, isum;
 	float bv[4];
 	int bi[4];
@@ -234,10 +240,15 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 	G.rank = threadIdx.x % TPP;
 	G.bar_id = 1 + local;
 	G.red = nullptr;
-	if (G.rank == 0) H.req = -1;
+	if (G.rank == 0) { H.req = -1; H.t_enter = global_ns(); H.t_task = 0; H.busy = 0; H.ntask = 0; }
 	G.sync();
 	for (;;) {
-		if (G.rank == 0) H.task = queue_pop(C);
+		if (G.rank == 0) {
+			if (H.t_task) H.busy += (unsigned long long)(global_ns() - H.t_task);
+			H.task = queue_pop(C);
+			H.t_task = H.task >= 0 ? global_ns() : 0;
+			H.ntask += H.task >= 0;
+		}
 		G.sync();
 		const int task = H.task;
 		if (task < 0) break;
@@ -347,6 +358,13 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 			atomicSub(&C.ctl->alive, 1);
 		}
 		G.sync();
+	}
+	if (G.rank == 0) {
+		atomicAdd(&C.ctl->busy_ns, H.busy);
+		atomicAdd(&C.ctl->tasks, H.ntask);
+		atomicAdd(&C.ctl->workers, 1);
+		atomicMin(&C.ctl->t_first, (unsigned long long)H.t_enter);
+		atomicMax(&C.ctl->t_last, (unsigned long long)global_ns());
 	}
 }
 
@@ -708,6 +726,7 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 			h_start[start[c] + i] = (1ull << 32) | task_word((uint32_t)(start[c] + i), kTaskStart, 0);
 		h_ctl[c].tail = work[c].size();
 		h_ctl[c].alive = (int)work[c].size();
+		h_ctl[c].t_first = ~0ull;
 	}
 	e = cudaMemcpyAsync(E.d_reqs, reqs.data(), sizeof(ReqDev) * reqs.size(), cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_work, all.data(), sizeof(RunRef) * nwork, cudaMemcpyHostToDevice, E.stream);
@@ -754,6 +773,11 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	for (int c = 0; c < NC; c++) {
 		if (h_ctl[c].err) return fail(ADGPU_ERR_TIMEOUT, "engine task queue: a reserved slot was never written");
 		if (h_ctl[c].alive != 0) return fail(ADGPU_ERR_STATE, "engine tick ended with runs still active");
+		if (h_ctl[c].workers > 0 && h_ctl[c].t_last > h_ctl[c].t_first) {
+			E.stats.worker_busy_s += 1e-9 * (double)h_ctl[c].busy_ns;
+			E.stats.worker_span_s += 1e-9 * (double)h_ctl[c].workers * (double)(h_ctl[c].t_last - h_ctl[c].t_first);
+			E.stats.tasks += h_ctl[c].tasks;
+		}
 	}
 	E.stats.ticks++;
 	// a request is complete when all its runs are

@@ -348,6 +348,11 @@ typedef struct {
 	uint64_t submitted, completed, ticks;
 	size_t   bytes_used, bytes_budget;
 	int      active;
+	/* Worker accounting over all ticks: time pose groups spent on tasks, and
+	 * pose groups x (first worker start .. last worker exit) per class and
+	 * tick; busy / span is the engine kernel's worker utilisation. */
+	double   worker_busy_s, worker_span_s;
+	uint64_t tasks;
 } adgpu_engine_stats;
 
 adgpu_status adgpu_engine_create(const adgpu_engine_config* cfg, adgpu_engine** out);
