@@ -343,6 +343,11 @@ def run_engine(args, rank, world, local_rank):
                 "clocks": clocks, "roofline": roof, "cost_model": cm}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(lig, args.lsmet)
+        if not args.no_batch:
+            # the batching comparison on a bounded sample of its configuration
+            bvp = run_batch(args)
+            line["batched_vs_plain"] = {k: bvp[k] for k in ("ligands", "nrun", "nev_per_run", "heavy_atoms", "batched",
+                                                            "plain", "batched_over_plain_ligands_per_hour", "tpp_classes")}
         del evals_per_docking
     return line
 
@@ -415,15 +420,22 @@ def run_batch(args):
     res = [en.result(i) for i in ids]
     t_batch = time.perf_counter() - t0
     ev_batch = sum(int(r.evals.sum()) for r in res)
+    st = en.stats()
+    util = st.worker_busy_s / st.worker_span_s if st.worker_span_s > 0 else None
     # plain: one ligand at a time through the kernel API, (a) driven by the
     # reference host's loop (a synchronous call per kernel per generation) --
     # the drop-in -- and (b) with the loop resident on the device
+    # sample: every k-th ligand; the plain rate is scaled to the whole set by
+    # per-ligand cost (pairs + 8 atoms per evaluation, the engine's weight)
     nplain = min(nlig, args.plain_sample)
+    sample = ligs[::max(1, nlig // nplain)][:nplain]
+    cost = lambda lg: lg.dockpars.num_of_intraE_contributors + 8.0 * lg.dockpars.num_of_atoms + 64.0  # noqa: E731
+    scale = sum(cost(lg) for lg in ligs) / sum(cost(lg) for lg in sample) * len(sample) / nlig
     ref_grid = grid.reference_layout()
     plain = {}
     for name, fn in (("reference_host_loop", dock.dock_host_loop), ("resident_loop", dock.dock)):
         t_plain, ev_plain = 0.0, 0
-        for lg in ligs[:nplain]:
+        for lg in sample:
             job = device.DeviceJob(lg.tables, lg.dockpars, ref_grid, nrun, lg.prng)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -433,12 +445,13 @@ def run_batch(args):
             t_plain += time.perf_counter() - t0
             ev_plain += int(r.evals_per_run.sum())
             del job
-        plain[name] = {"ligands_sampled": nplain, "seconds": t_plain, "ligands_per_hour": 3600.0 * nplain / t_plain,
-                       "evals_per_s": ev_plain / t_plain}
+        plain[name] = {"ligands_sampled": nplain, "seconds": t_plain, "ligands_per_hour": 3600.0 * nplain / t_plain / scale,
+                       "evals_per_s": ev_plain / t_plain, "sample_cost_scale": scale}
     lph_b = 3600.0 * nlig / t_batch
     return {"mode": "batch", "ligands": nlig, "nrun": nrun, "nev_per_run": nev, "lsmet": args.lsmet,
             "heavy_atoms": [min(a for a, _ in sizes), max(a for a, _ in sizes)],
-            "batched": {"seconds": t_batch, "ligands_per_hour": lph_b, "evals_per_s": ev_batch / t_batch},
+            "batched": {"seconds": t_batch, "ligands_per_hour": lph_b, "evals_per_s": ev_batch / t_batch,
+                        "worker_utilisation": util, "tasks": int(st.tasks)},
             "plain": plain,
             "batched_over_plain_ligands_per_hour": {k: lph_b / v["ligands_per_hour"] for k, v in plain.items()},
             "tpp_classes": tpps}
@@ -526,6 +539,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--lsmet", default="ad", choices=["ad", "sw", "adam", "fire"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain sample in the default mode")
     ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel", "batch", "serve"])
     ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel mode)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
