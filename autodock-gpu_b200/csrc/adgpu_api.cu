@@ -165,14 +165,15 @@ adgpu_status launch_lga(const KArgs& a, float* grads, cudaStream_t stream, int c
 	return ADGPU_OK;
 }
 
-// Threads per pose for a launch of n blocks when none is configured: 64 when
-// every block still gets a resident pose group of 64 threads (6 CTAs of 128
-// threads per SM), else 32.  A per-ligand launch of a few runs has few
-// local-search entities, and two warps per pose then shorten each entity's
-// chain of evaluations; on B200, 64 beat both 32 and 128 for per-ligand
-// dockings of 20 and of 100 runs (10-64 heavy atoms).
-static int auto_tpp(uint32_t n)
+// Threads per pose for a launch of n blocks when none is configured.  Local
+// searches: 64.  A local-search launch ends with its longest entities running
+// alone, and two warps per pose halve that tail; on B200, 64 beat 32 and 128
+// for per-ligand dockings of 20 and of 100 runs (80% local-search rate,
+// 10-64 heavy atoms).  Other kernels: 64 when every block still gets a
+// resident pose group of 64 threads (6 CTAs of 128 threads per SM), else 32.
+static int auto_tpp(uint32_t n, bool local_search)
 {
+	if (local_search) return 64;
 	if (g_num_sms == 0) {
 		int dev = 0;
 		if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -185,7 +186,7 @@ static int auto_tpp(uint32_t n)
 template <int KIND>
 adgpu_status launch_kind(const KArgs& a, float* grads, cudaStream_t stream, int tpp)
 {
-	if (tpp == 0) tpp = auto_tpp(a.nblocks);
+	if (tpp == 0) tpp = auto_tpp(a.nblocks, KIND >= 1 && KIND <= 4);
 	switch (tpp) {
 	case 32: return launch_lga<32, KIND>(a, grads, stream, 128);
 	case 64: return launch_lga<64, KIND>(a, grads, stream, 128);

@@ -321,6 +321,7 @@ def run_engine(args, rank, world, local_rank):
                 traffic = None
         roof = {"bound": "fp32", "achieved": achieved, "peak": float(peak.value), "unit": "TFLOP/s",
                 "frac": achieved / float(peak.value), "traffic": traffic,
+                "traffic_source": "ncu dram bytes per launch of this launch shape (profiles/ls_kernel_traffic.json)",
                 "peak_source": "measured in this run (FMA-chain probe, adgpu_measure_fp32_peak); "
                                "MEASURED_PEAKS.json has no FP32 figure",
                 "kernel": entry, "launch_ms": dur * 1e3, "evals_per_launch": statistics.mean(ls_evals),
@@ -363,9 +364,9 @@ def run_kernel_only(args):
     w = WORKLOAD
     nrun = args.nrun or w["nrun"]
     job = device.DeviceJob(lig.tables, lig.dockpars, ref_grid, nrun, lig.prng)
-    # the docking that produces the population runs with 64 threads per pose
-    # so that a profiler can select the measured 32-thread launches by name
-    os.environ["ADGPU_THREADS_PER_POSE"] = "64"
+    # the docking that produces the population runs with another group size
+    # than the measured launches, so that a profiler can select them by name
+    os.environ["ADGPU_THREADS_PER_POSE"] = "32" if args.tpp == 64 else "64"
     job.activate()
     init_dev = torch.from_numpy(lig.initpop[:nrun * w["pop"]]).cuda()
     mid = dock.dock(job, init_dev, args.lsmet, w["nev"], 10)
