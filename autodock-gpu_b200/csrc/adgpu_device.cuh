@@ -270,6 +270,137 @@ __device__ __forceinline__ GenRot genrot_of(const float* g, bool has_ligand)
 	return r;
 }
 
+// ---- intramolecular pairs, two per thread with packed FP32 -------------------------
+// sm_100 executes FADD2/FMUL2/FFMA2: one instruction on two floats.  The pair
+// loop is issue bound, so each thread takes two pairs per iteration and runs
+// their shared arithmetic packed; compares, selects, reciprocals and the
+// fixed-point atomics stay per pair.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 f2neg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// inv^e by squaring (the general-exponent path of modified pair potentials)
+static __device__ __noinline__ float pow_int(float b, int e)
+{
+	float r = 1.0f;
+	while (e) { if (e & 1) r *= b; b *= b; e >>= 1; }
+	return r;
+}
+
+// Energy of the pairs this thread takes (rank, rank + TPP, rank + 2*TPP, ...),
+// with, for GRAD, their fixed-point forces added to S.fx/fy/fz.  The terms
+// are the reference's (cuda/calcMergeEneGra.cu:418-602) rewritten with one
+// reciprocal square root and three reciprocals per pair instead of divisions
+// and __powf:  (AC - sd^(m-n) BD) sd^-m = AC/sd^m - BD/sd^n  (m = 12, n = 6 or 10).
+template <int TPP, bool GRAD>
+__device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, int rank)
+{
+	constexpr uint32_t k12_6 = 12u | (6u << 8), k12_10 = 12u | (10u << 8);
+	const float hs = L.half_smooth, emd = L.elec_min_distance;
+	const float inv_emd = __fdividef(1.0f, emd);
+	float2 esum = f2s(0.0f);
+	for (int p = rank; p < L.npairs; p += 2 * TPP) {
+		const bool has_b = p + TPP < L.npairs;       // the second pair; else pair a twice, b discarded
+		const float4* pra = reinterpret_cast<const float4*>(L.pairs + p);
+		const float4* prb = reinterpret_cast<const float4*>(L.pairs + (has_b ? p + TPP : p));
+		const float4 Aa = __ldg(pra), Ba = __ldg(pra + 1), Ab = __ldg(prb), Bb = __ldg(prb + 1);
+		const uint32_t ija = __float_as_uint(Ba.z), ijb = __float_as_uint(Bb.z);
+		const int a1 = ija & 0xFF, a2 = (ija >> 8) & 0xFF, b1 = ijb & 0xFF, b2 = (ijb >> 8) & 0xFF;
+		const float4 pa1 = S.xyz[a1], pa2 = S.xyz[a2], pb1 = S.xyz[b1], pb2 = S.xyz[b2];
+		const float2 sx = f2add(f2(pa1.x, pb1.x), f2(-pa2.x, -pb2.x));
+		const float2 sy = f2add(f2(pa1.y, pb1.y), f2(-pa2.y, -pb2.y));
+		const float2 sz = f2add(f2(pa1.z, pb1.z), f2(-pa2.z, -pb2.z));
+		const float2 d2g = f2fma(sz, sz, f2fma(sy, sy, f2mul(sx, sx)));
+		const float2 inv_dist = f2(rsqrtf(d2g.x), rsqrtf(d2g.y));
+		float2 r = f2mul(d2g, inv_dist);
+		r.x = d2g.x > 0.0f ? r.x : 0.0f;
+		r.y = d2g.y > 0.0f ? r.y : 0.0f;
+		r = f2mul(r, f2s(L.spacing));
+		const float2 vbond = f2(Ba.y, Bb.y);          // G for CG-G0 pairs, else 0
+		float2 e = f2mul(vbond, r);
+		float2 pg = vbond;
+		// vdW / H-bond, cut-off 8 A
+		{
+			const float2 reqm = f2(Aa.z, Ab.z);
+			const float2 delta = f2add(reqm, f2neg(r));
+			float2 sd;
+			sd.x = fabsf(delta.x) >= hs ? r.x + copysignf(hs, delta.x) : reqm.x;
+			sd.y = fabsf(delta.y) >= hs ? r.y + copysignf(hs, delta.y) : reqm.y;
+			const float2 inv = f2(__fdividef(1.0f, sd.x), __fdividef(1.0f, sd.y));
+			const float2 i2 = f2mul(inv, inv), i4 = f2mul(i2, i2), i6 = f2mul(i4, i2);
+			float2 im = f2mul(i6, i6), in_, fm = f2s(12.0f), fn;
+			const uint32_t mna = ija >> 16, mnb = ijb >> 16;
+			if ((mna == k12_6 || mna == k12_10) && (mnb == k12_6 || mnb == k12_10)) {
+				const float2 i10 = f2mul(i6, i4);
+				in_.x = mna == k12_10 ? i10.x : i6.x;
+				in_.y = mnb == k12_10 ? i10.y : i6.y;
+				fn.x = mna == k12_10 ? 10.0f : 6.0f;
+				fn.y = mnb == k12_10 ? 10.0f : 6.0f;
+			} else {
+				const int ma = mna & 0xFF, na = mna >> 8, mb = mnb & 0xFF, nb = mnb >> 8;
+				im = f2(pow_int(inv.x, ma), pow_int(inv.y, mb));
+				in_ = f2(pow_int(inv.x, na), pow_int(inv.y, nb));
+				fm = f2((float)ma, (float)mb);
+				fn = f2((float)na, (float)nb);
+			}
+			const float2 ac = f2(Aa.x, Ab.x), bd = f2(Aa.y, Ab.y);
+			const float2 bd_in = f2mul(bd, in_), ac_im = f2mul(ac, im);
+			const float2 ev = f2add(ac_im, f2neg(bd_in));
+			const bool ca = r.x < 8.0f, cb = r.y < 8.0f;
+			e = f2add(e, f2(ca ? ev.x : 0.0f, cb ? ev.y : 0.0f));
+			if (GRAD) {
+				const float2 gv = f2mul(f2add(f2mul(fn, bd_in), f2neg(f2mul(fm, ac_im))), inv);
+				pg = f2add(pg, f2(ca ? gv.x : 0.0f, cb ? gv.y : 0.0f));
+			}
+		}
+		// electrostatics and desolvation, cut-off 20.48 A
+		{
+			const bool ca = r.x < 20.48f, cb = r.y < 20.48f;
+			float2 inv_r = f2mul(inv_dist, f2s(L.inv_spacing));
+			float2 rr = r;
+			if (rr.x < emd) { rr.x = emd; inv_r.x = inv_emd; }
+			if (rr.y < emd) { rr.y = emd; inv_r.y = inv_emd; }
+			const float2 d2 = f2mul(rr, rr);
+			const float2 num = f2fma(f2mul(f2s(-0.1063f), d2), f2fma(f2s(-0.001947f), d2, f2s(1.0f)), f2s(12.96f));
+			const float2 den = f2fma(d2, f2fma(d2, f2fma(f2s(0.000112f), d2, f2s(0.00357f)), f2s(0.4137f)), f2s(12.96f));
+			const float2 cn = f2mul(f2s(L.coeff_desolv), num);
+			const float2 desolv = f2mul(f2(Aa.w, Ab.w), f2(__fdividef(cn.x, den.x), __fdividef(cn.y, den.y)));
+			const float2 rs = f2(__fdividef(1.0f, rr.x + 1.26366f), __fdividef(1.0f, rr.y + 1.26366f));
+			const float2 rs2 = f2mul(rs, rs);
+			const float2 diel = f2fma(f2s(1.10859f), rs2, f2s(0.010358f));
+			const float2 es = f2mul(f2(Ba.x, Bb.x), inv_r);
+			const float2 ee = f2fma(diel, es, desolv);
+			e = f2add(e, f2(ca ? ee.x : 0.0f, cb ? ee.y : 0.0f));
+			if (GRAD) {
+				const float2 t1 = f2mul(f2mul(es, inv_r), diel);
+				const float2 t2 = f2mul(f2mul(f2mul(es, f2s(2.21718f)), rs2), rs);
+				const float2 t3 = f2mul(f2mul(f2s(0.0771605f), rr), desolv);
+				const float2 ge = f2add(f2add(t1, t2), t3);
+				pg = f2add(pg, f2(ca ? -ge.x : 0.0f, cb ? -ge.y : 0.0f));
+			}
+		}
+		esum = f2add(esum, f2(e.x, has_b ? e.y : 0.0f));
+		if (GRAD) {
+			// fixed-point forces; the 1024 scale folded into gdd (a power of two:
+			// the same rounding as quant(sub * gdd))
+			const float2 gdd = f2mul(f2mul(f2neg(pg), inv_dist), f2s(kTermScale));
+			const float2 gx = f2mul(sx, gdd), gy = f2mul(sy, gdd), gz = f2mul(sz, gdd);
+			int ix = quant_scaled(gx.x), iy = quant_scaled(gy.x), iz = quant_scaled(gz.x);
+			atomicAdd(&S.fx[a1], -ix); atomicAdd(&S.fy[a1], -iy); atomicAdd(&S.fz[a1], -iz);
+			atomicAdd(&S.fx[a2], ix); atomicAdd(&S.fy[a2], iy); atomicAdd(&S.fz[a2], iz);
+			if (has_b) {
+				ix = quant_scaled(gx.y); iy = quant_scaled(gy.y); iz = quant_scaled(gz.y);
+				atomicAdd(&S.fx[b1], -ix); atomicAdd(&S.fy[b1], -iy); atomicAdd(&S.fz[b1], -iz);
+				atomicAdd(&S.fx[b2], ix); atomicAdd(&S.fy[b2], iy); atomicAdd(&S.fz[b2], iz);
+			}
+		}
+	}
+	return esum.x + esum.y;
+}
+
 // ---- the scorer -----------------------------------------------------------------------
 // Scores genotype g (shared memory, read-only here).  Returns the energy (same
 // value in every thread of the group).  With GRAD, writes dE/dgene to
@@ -377,66 +508,7 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	G.sync();
 
 	// 4. intramolecular pairs (cuda/calcMergeEneGra.cu:418-602)
-	// The reference's terms, rewritten with one reciprocal square root and two
-	// reciprocals per pair instead of divisions and __powf:
-	//   (AC - sd^(m-n) BD) sd^-m = AC/sd^m - BD/sd^n  (m = 12, n = 6 or 10)
-	for (int p = rank; p < L.npairs; p += TPP) {
-		const float4* pr = reinterpret_cast<const float4*>(L.pairs + p);
-		float4 A = __ldg(pr), B = __ldg(pr + 1);
-		uint32_t ij = __float_as_uint(B.z);
-		int a1 = ij & 0xFF, a2 = (ij >> 8) & 0xFF;
-		const float4 p1 = S.xyz[a1], p2 = S.xyz[a2];
-		float subx = p1.x - p2.x, suby = p1.y - p2.y, subz = p1.z - p2.z;
-		float d2g = subx * subx + suby * suby + subz * subz;
-		float inv_dist = rsqrtf(d2g);
-		float dist = d2g > 0.0f ? d2g * inv_dist : 0.0f;
-		float r = dist * L.spacing;
-		float pg = B.y;                       // vbond (G for CG-G0 pairs)
-		e_acc += B.y * r;
-		if (r < 8.0f) {
-			float delta = A.z - r;
-			float sd = (fabsf(delta) >= L.half_smooth) ? r + copysignf(L.half_smooth, delta) : A.z;
-			float inv = __fdividef(1.0f, sd);
-			float i2 = inv * inv, i4 = i2 * i2, i6 = i4 * i2, i12 = i6 * i6;
-			uint32_t mn = ij >> 16;           // m | n << 8
-			float im, in_, fm, fn;
-			if (mn == (12u | (6u << 8))) { im = i12; in_ = i6; fm = 12.0f; fn = 6.0f; }
-			else if (mn == (12u | (10u << 8))) { im = i12; in_ = i6 * i4; fm = 12.0f; fn = 10.0f; }
-			else {
-				// general exponents (modified pair potentials): inv^m, inv^n by squaring
-				int m = mn & 0xFF, n = mn >> 8;
-				im = 1.0f; in_ = 1.0f;
-				float b = inv; int e = m;
-				while (e) { if (e & 1) im *= b; b *= b; e >>= 1; }
-				b = inv; e = n;
-				while (e) { if (e & 1) in_ *= b; b *= b; e >>= 1; }
-				fm = (float)m; fn = (float)n;
-			}
-			e_acc += A.x * im - A.y * in_;
-			if (GRAD) pg += (fn * A.y * in_ - fm * A.x * im) * inv;
-		}
-		if (r < 20.48f) {
-			float inv_r = inv_dist * L.inv_spacing;
-			if (r < L.elec_min_distance) { r = L.elec_min_distance; inv_r = __fdividef(1.0f, r); }
-			float d2 = r * r;
-			float desolv = A.w * __fdividef(L.coeff_desolv * (12.96f - 0.1063f * d2 * (1.0f - 0.001947f * d2)),
-			                                (12.96f + d2 * (0.4137f + d2 * (0.00357f + 0.000112f * d2))));
-			float rs = __fdividef(1.0f, r + 1.26366f);
-			float rs2 = rs * rs;
-			float diel = 1.10859f * rs2 + 0.010358f;
-			float es = B.x * inv_r;
-			e_acc += diel * es + desolv;
-			if (GRAD) pg += -(es * inv_r) * diel - es * 2.21718f * rs2 * rs - 0.0771605f * r * desolv;
-		}
-		if (GRAD) {
-			// quant(sub * gdd) with the 1024 scale folded into gdd (a power of
-			// two: the same rounding, one multiply instead of three)
-			const float gdd = -pg * inv_dist * kTermScale;
-			const int ix = quant_scaled(subx * gdd), iy = quant_scaled(suby * gdd), iz = quant_scaled(subz * gdd);
-			atomicSub(&S.fx[a1], ix); atomicSub(&S.fy[a1], iy); atomicSub(&S.fz[a1], iz);
-			atomicAdd(&S.fx[a2], ix); atomicAdd(&S.fy[a2], iy); atomicAdd(&S.fz[a2], iz);
-		}
-	}
+	e_acc += pair_terms<TPP, GRAD>(L, S, rank);
 	const float energy = G.sum(e_acc);
 	if (!GRAD) return energy;
 	G.sync();
