@@ -409,6 +409,12 @@ def make_flexres(seed: int, n_atoms: int, n_torsions: int, anchor: np.ndarray) -
 
 def write_flexres(residues: list, path: str) -> None:
     """Writes flexible residues (list of Molecule) in the AutoDock flexres format."""
+    with open(path, "w") as f:
+        f.write(flexres_text(residues))
+
+
+def flexres_text(residues: list) -> str:
+    """Flexible residues (list of Molecule) as AutoDock flexres PDBQT text."""
     out = []
     serial = 1
     for k, mol in enumerate(residues):
@@ -420,8 +426,7 @@ def write_flexres(residues: list, path: str) -> None:
         out.extend(lines)
         out.append(f"END_RES {resname} {chain}{resseq:4d}")
         serial += len(order)
-    with open(path, "w") as f:
-        f.write("\n".join(out) + "\n")
+    return "\n".join(out) + "\n"
 
 
 # --------------------------------------------------------------------------

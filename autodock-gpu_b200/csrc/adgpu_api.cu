@@ -9,6 +9,7 @@
 #include <mutex>
 
 #include "adgpu_kernels.cuh"
+#include "adgpu_autostop.cuh"
 #include "adgpu_tables.h"
 
 #ifndef ADGPU_MIN_CTAS
@@ -87,22 +88,47 @@ __global__ void sum_evals_kernel(const int* evals_new, int* evals_runs, int pop_
 // Stop test of the resident docking loop (check_progress,
 // host/src/performdocking.cpp.Cuda:908-942): stop when the mean evals per run
 // reach max_evals or the generation count reaches max_gens.
-__global__ void progress_kernel(const int* evals_runs, int runs, unsigned long long max_evals,
-                                unsigned int max_gens, unsigned int* gen_counter, int* stop_flag)
+// With AutoStop (as != nullptr), a generation count that is a multiple of
+// as_frequency also runs the AutoStop check on the current energies and stops
+// once it is satisfied and the evaluations exceed min_as_evals
+// (performdocking.cpp.Cuda:689-698).  Launch with 256 threads.
+struct AutoStopArgs {
+	AutoStopState* state;        // nullptr: no AutoStop
+	float* stats;                // (pop_size + 1) * 3
+	float* buf_e;                // R * P
+	uint16_t* buf_m;             // R * P
+	const float* energies;       // the population about to be bred
+	unsigned long long min_evals;
+};
+
+__global__ void __launch_bounds__(256) progress_kernel(const int* evals_runs, int runs, unsigned long long max_evals,
+                                                       unsigned int max_gens, unsigned int* gen_counter, int* stop_flag,
+                                                       AutoStopArgs as)
 {
 	if (*stop_flag) return;
 	__shared__ unsigned long long tot;
+	__shared__ int s_stop;
+	__shared__ int s_count[257];
+	__shared__ float s_best[256];
 	if (threadIdx.x == 0) tot = 0;
 	__syncthreads();
 	unsigned long long s = 0;
 	for (int i = threadIdx.x; i < runs; i += blockDim.x) s += (unsigned long long)evals_runs[i];
 	atomicAdd(&tot, s);
 	__syncthreads();
+	const unsigned int g = *gen_counter;
 	if (threadIdx.x == 0) {
-		unsigned int g = *gen_counter;
 		double ev = (double)tot / (double)runs / (double)max_evals * 100.0;
 		double gp = (double)g / (double)max_gens * 100.0;
-		if ((ev > gp ? ev : gp) >= 100.0) *stop_flag = 1;
+		s_stop = (ev > gp ? ev : gp) >= 100.0;
+	}
+	__syncthreads();
+	if (!s_stop && as.state && g % as.state->as_frequency == 0) {
+		autostop_check(*as.state, as.stats, as.buf_e, as.buf_m, as.energies, (int)g, s_count, s_best);
+		if (threadIdx.x == 0 && as.state->autostopped && tot > as.min_evals) s_stop = 1;
+	}
+	if (threadIdx.x == 0) {
+		if (s_stop) *stop_flag = 1;
 		else *gen_counter = g + 1;
 	}
 }
@@ -239,7 +265,9 @@ adgpu_status check_threads(uint32_t threads)
 // and two generations (A->B, B->A) captured in one CUDA graph, so the host
 // only launches graphs and polls a pinned stop flag every few generations.
 adgpu_status dock_resident(ApiState& s, int lsmet, uint32_t runs, uint64_t max_evals, uint32_t max_gens,
-                           float* c1, float* e1, float* c2, float* e2, int* final_is_second, uint32_t* generations)
+                           uint32_t as_frequency, float stopstd, uint64_t min_as_evals,
+                           float* c1, float* e1, float* c2, float* e2, int* final_is_second, uint32_t* generations,
+                           int* autostopped)
 {
 	const adgpu_dockpars& dp = s.data.dockpars;
 	const uint32_t T = 64;
@@ -247,6 +275,7 @@ adgpu_status dock_resident(ApiState& s, int lsmet, uint32_t runs, uint64_t max_e
 	ADGPU_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
 	int* d_flag = nullptr; unsigned int* d_gen = nullptr;
 	int* h_flag = nullptr;
+	char* d_as = nullptr;                // AutoStop state, statistics and buffers
 	cudaGraph_t graph = nullptr; cudaGraphExec_t exec = nullptr;
 	adgpu_status rc = ADGPU_OK;
 	auto cleanup = [&]() {
@@ -254,6 +283,7 @@ adgpu_status dock_resident(ApiState& s, int lsmet, uint32_t runs, uint64_t max_e
 		if (graph) cudaGraphDestroy(graph);
 		if (d_flag) cudaFree(d_flag);
 		if (d_gen) cudaFree(d_gen);
+		if (d_as) cudaFree(d_as);
 		if (h_flag) cudaFreeHost(h_flag);
 		cudaStreamDestroy(st);
 	};
@@ -263,6 +293,21 @@ adgpu_status dock_resident(ApiState& s, int lsmet, uint32_t runs, uint64_t max_e
 	ADGPU_TRY(cudaMallocHost(&h_flag, sizeof(int)), "pinned flag");
 	ADGPU_TRY(cudaMemsetAsync(d_flag, 0, sizeof(int), st), "flag init");
 	ADGPU_TRY(cudaMemsetAsync(d_gen, 0, sizeof(unsigned int), st), "gen init");
+	AutoStopArgs as_args{};
+	if (as_frequency > 0) {
+		const size_t n = (size_t)runs * dp.pop_size;
+		const size_t o_stats = 256, o_e = o_stats + autostop_stats_floats(dp.pop_size) * 4;
+		const size_t o_m = (o_e + n * 4 + 15) / 16 * 16, bytes = o_m + n * 2 + 16;
+		ADGPU_TRY(cudaMalloc(&d_as, bytes), "autostop state");
+		AutoStopState h;
+		autostop_init(h, dp.pop_size, (int)runs, stopstd, as_frequency);
+		ADGPU_TRY(cudaMemcpyAsync(d_as, &h, sizeof(h), cudaMemcpyHostToDevice, st), "autostop init");
+		as_args.state = reinterpret_cast<AutoStopState*>(d_as);
+		as_args.stats = reinterpret_cast<float*>(d_as + o_stats);
+		as_args.buf_e = reinterpret_cast<float*>(d_as + o_e);
+		as_args.buf_m = reinterpret_cast<uint16_t*>(d_as + o_m);
+		as_args.min_evals = min_as_evals;
+	}
 	KArgs a = make_args(s);
 	a.ref_threads = T;
 	a.stop_flag = d_flag;
@@ -271,7 +316,10 @@ adgpu_status dock_resident(ApiState& s, int lsmet, uint32_t runs, uint64_t max_e
 	for (int half = 0; half < 2; half++) {
 		float* cc = half ? c2 : c1; float* ec = half ? e2 : e1;
 		float* cn = half ? c1 : c2; float* en = half ? e1 : e2;
-		progress_kernel<<<1, 256, 0, st>>>(s.data.pMem_gpu_evals_of_runs, (int)runs, (unsigned long long)max_evals, max_gens, d_gen, d_flag);
+		AutoStopArgs ash = as_args;
+		ash.energies = ec;
+		progress_kernel<<<1, 256, 0, st>>>(s.data.pMem_gpu_evals_of_runs, (int)runs, (unsigned long long)max_evals, max_gens,
+		                                   d_gen, d_flag, ash);
 		KArgs g = a;
 		g.nblocks = runs * (uint32_t)dp.pop_size;
 		g.conf_cur = cc; g.e_cur = ec; g.conf = cn; g.e = en;
@@ -306,6 +354,12 @@ adgpu_status dock_resident(ApiState& s, int lsmet, uint32_t runs, uint64_t max_e
 	ADGPU_TRY(cudaMemcpy(&g, d_gen, sizeof(g), cudaMemcpyDeviceToHost), "gen read");
 	*generations = g;
 	*final_is_second = (int)(g & 1u);
+	*autostopped = 0;
+	if (as_args.state) {
+		AutoStopState h;
+		ADGPU_TRY(cudaMemcpy(&h, as_args.state, sizeof(h), cudaMemcpyDeviceToHost), "autostop read");
+		*autostopped = h.autostopped;
+	}
 	cleanup();
 #undef ADGPU_TRY
 	return ADGPU_OK;
@@ -435,7 +489,25 @@ adgpu_status adgpu_dock_resident(int lsmet, uint32_t num_runs, uint64_t max_eval
 	if (lsmet < 0 || lsmet > 3) return fail(ADGPU_ERR_ARG, "lsmet must be 0 (sw), 1 (ad), 2 (adam) or 3 (fire)");
 	if (!c1 || !e1 || !c2 || !e2 || !final_is_second || !generations) return fail(ADGPU_ERR_ARG, "null buffer");
 	if (num_runs == 0 || num_runs > ADGPU_MAX_RUNS || max_evals == 0 || max_gens == 0) return fail(ADGPU_ERR_ARG, "bad run limits");
-	return dock_resident(s, lsmet, num_runs, max_evals, max_gens, c1, e1, c2, e2, final_is_second, generations);
+	int as = 0;
+	return dock_resident(s, lsmet, num_runs, max_evals, max_gens, 0, 0.0f, 0, c1, e1, c2, e2, final_is_second, generations, &as);
+}
+
+adgpu_status adgpu_dock_resident_autostop(int lsmet, uint32_t num_runs, uint64_t max_evals, uint32_t max_gens,
+                                          uint32_t as_frequency, float stopstd, uint64_t min_as_evals,
+                                          float* c1, float* e1, float* c2, float* e2,
+                                          int* final_is_second, uint32_t* generations, int* autostopped)
+{
+	ApiState& s = api();
+	if (!s.ready) return fail(ADGPU_ERR_NOT_READY, "adgpu_set_kernels_gpu_data not called");
+	if (lsmet < 0 || lsmet > 3) return fail(ADGPU_ERR_ARG, "lsmet must be 0 (sw), 1 (ad), 2 (adam) or 3 (fire)");
+	if (!c1 || !e1 || !c2 || !e2 || !final_is_second || !generations || !autostopped) return fail(ADGPU_ERR_ARG, "null buffer");
+	if (num_runs == 0 || num_runs > ADGPU_MAX_RUNS || max_evals == 0 || max_gens == 0) return fail(ADGPU_ERR_ARG, "bad run limits");
+	if (as_frequency == 0) return fail(ADGPU_ERR_ARG, "as_frequency must be at least 1");
+	if (!(stopstd > 0.0f)) return fail(ADGPU_ERR_ARG, "stopstd must be positive");
+	if (s.data.dockpars.pop_size < 11) return fail(ADGPU_ERR_ARG, "AutoStop needs a population of at least 11");
+	return dock_resident(s, lsmet, num_runs, max_evals, max_gens, as_frequency, stopstd, min_as_evals,
+	                     c1, e1, c2, e2, final_is_second, generations, autostopped);
 }
 
 }  // extern "C"

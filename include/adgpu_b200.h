@@ -263,6 +263,22 @@ adgpu_status adgpu_dock_resident(int lsmet, uint32_t num_runs, uint64_t max_eval
                                  float* conformations2, float* energies2,
                                  int* final_is_second, uint32_t* generations);
 
+/* adgpu_dock_resident with the reference's AutoStop (--autostop 1,
+ * host/inc/autostop.hpp:169-222, applied as in
+ * host/src/performdocking.cpp.Cuda:689-698): every `as_frequency`
+ * generations (--asfreq) the convergence test runs on the device on the
+ * current energies, and the loop ends once it is satisfied (standard
+ * deviation of the best energies below `stopstd`, --stopstd) and the total
+ * evaluations exceed `min_as_evals` (the reference's heuristics minimum; 0
+ * without heuristics).  *autostopped reports whether it triggered.  The
+ * reference copies all energies to the host for each test; here nothing
+ * leaves the device until the loop ends. */
+adgpu_status adgpu_dock_resident_autostop(int lsmet, uint32_t num_runs, uint64_t max_evals, uint32_t max_gens,
+                                          uint32_t as_frequency, float stopstd, uint64_t min_as_evals,
+                                          float* conformations1, float* energies1,
+                                          float* conformations2, float* energies2,
+                                          int* final_is_second, uint32_t* generations, int* autostopped);
+
 /* ---------------------------------------------------------------------------
  * Front end: the input side of the path.  Reads AutoDock-4 grid maps and
  * prepares PDBQT ligands (with optional flexible residues) into the

@@ -57,8 +57,30 @@ def lib():
         L.adgpu_ref_gen_and_eval_newpops.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp, vp]
         for n in ("perform_ls", "gradient_minad", "gradient_minadam"):
             getattr(L, f"adgpu_ref_{n}").argtypes = [C.c_uint32, C.c_uint32, vp, vp]
+        L.adgpu_ref_autostop_new.restype = vp
+        L.adgpu_ref_autostop_new.argtypes = [C.c_int, C.c_int, C.c_float, C.c_int]
+        L.adgpu_ref_autostop_check.restype = C.c_int
+        L.adgpu_ref_autostop_check.argtypes = [vp, C.c_int, vp, C.c_ulong]
+        L.adgpu_ref_autostop_free.argtypes = [vp]
         _lib = L
     return _lib
+
+
+class RefAutoStop:
+    """The reference's own AutoStop object (host/inc/autostop.hpp, compiled
+    into _ref/libadgpu_ref.so by ref/ref_autostop.cpp)."""
+
+    def __init__(self, pop_size: int, num_runs: int, stopstd: float, as_frequency: int):
+        self.h = lib().adgpu_ref_autostop_new(pop_size, num_runs, stopstd, as_frequency)
+
+    def check(self, generation: int, energies: np.ndarray, total_evals: int) -> bool:
+        e = np.ascontiguousarray(energies, np.float32)
+        return bool(lib().adgpu_ref_autostop_check(self.h, generation, e.ctypes.data_as(C.c_void_p), total_evals))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().adgpu_ref_autostop_free(self.h)
+            self.h = None
 
 
 def _ptr(a):
