@@ -24,7 +24,7 @@ def ligand(grid, idx, n_heavy, n_tors, runs=4, pop=150):
                            num_runs=runs)
 
 
-@pytest.mark.parametrize("lsmet", ["ad", "sw"])
+@pytest.mark.parametrize("lsmet", ["ad", "sw", "adam", "fire"])
 def test_engine_matches_plain_path(grid, lsmet, monkeypatch):
     """With a generation budget both paths stop at the same generation, so the
     run must come out identical (same kernels, same PRNG states).  One run:
@@ -125,3 +125,37 @@ def test_continuous_admission_and_budget(grid):
     small.result(a)
     assert small.submit(ligs[1], rec, "ad", max_evals=nev, raise_on_budget=False) is not None
     torch.cuda.synchronize()
+
+
+def test_ga_only_and_mixed_population_sizes(grid, monkeypatch):
+    """Edge cases of the task queues: a request without local search (rate 0:
+    only GA phases) next to requests of population 50 and 150 in one tick,
+    each identical to its plain-path docking."""
+    monkeypatch.setenv("ADGPU_THREADS_PER_POSE", "32")
+    gens = 5
+    specs = [(0, 150, 0.0), (1, 50, 100.0), (2, 150, 100.0)]
+    ligs = []
+    for idx, pop, rate in specs:
+        run = frontend.default_dockpars(grid.spacing, pop)
+        run.lsearch_rate = rate
+        run.num_of_lsentities = int(rate / 100.0 * pop + 0.5)   # as the reference derives it
+        mol = synth.ligand_for(3, 40 + idx, 14 + 3 * idx, 3)
+        text = "\n".join(synth.pdbqt_lines(mol)[0]) + "\n"
+        ligs.append(frontend.Ligand(grid, text, None, run=run, seed=SEED, num_runs=1))
+    plain = []
+    for lg in ligs:
+        job = device.DeviceJob(lg.tables, lg.dockpars, grid.reference_layout(), 1, lg.prng)
+        job.activate()
+        res = dock.dock(job, lg.initpop, "ad", nev=10**9, ngen=gens)
+        plain.append((res.evals_per_run.copy(), float(res.energies.min().item())))
+    en = engine.Engine(threads_per_pose=32)
+    rec = en.add_receptor(grid)
+    ids = [en.submit(lg, rec, "ad", max_evals=10**12, max_gens=gens) for lg in ligs]
+    en.run()
+    for rid, (ev, best), (idx, pop, rate) in zip(ids, plain, specs):
+        r = en.result(rid)
+        assert np.all(r.generations == gens)
+        np.testing.assert_array_equal(r.evals, ev)
+        assert r.best_energies[0] == best
+        if rate == 0.0:
+            assert int(r.evals[0]) == pop * (gens + 1) - gens    # GA only: P per generation minus the elite

@@ -66,3 +66,19 @@ def test_out_of_grid_penalty(cases):
     assert np.all(e_gpu[:32] > 1.6e7)
     assert np.allclose(e_gpu, e_ref, rtol=1e-5)
     assert np.allclose(gr_gpu[:32, :3], gr_ref[:32, :3])
+
+
+def test_large_ligand_parity(tmp_path):
+    """Near the reference's limits: 110 heavy atoms (plus polar H), 30
+    torsions, some 6,400 intramolecular pairs."""
+    from adgpu_b200 import device
+    case = helpers.make_case(str(tmp_path / "big"), 60, ["C", "A", "N", "OA", "HD"], 110, 30, 2, config_id=2,
+                             lig_index=7)
+    dj = _activate(case)
+    g = helpers.in_box_genotypes(case, 300, seed=3)
+    e_gpu, gr_gpu = device.score(g, True)
+    e_ref, gr_ref = case.host.score(g, True, nthreads=8)
+    assert np.all(np.abs(e_gpu - e_ref) <= helpers.energy_tolerance(e_ref)), np.abs(e_gpu - e_ref).max()
+    ng = case.ngenes
+    assert np.all(np.abs(gr_gpu[:, :ng] - gr_ref[:, :ng]) <= helpers.gradient_bound(case, gr_ref))
+    del dj
