@@ -281,6 +281,13 @@ __device__ __forceinline__ float2 f2neg(float2 a) { return make_float2(-a.x, -a.
 __device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// 1.0f where a < b, else 0.0f (one FSET, no predicate and select)
+__device__ __forceinline__ float lt1(float a, float b)
+{
+	float r;
+	asm("set.lt.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+	return r;
+}
 
 // inv^e by squaring (the general-exponent path of modified pair potentials)
 static __device__ __noinline__ float pow_int(float b, int e)
@@ -314,11 +321,9 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 		const float2 sy = f2add(f2(pa1.y, pb1.y), f2(-pa2.y, -pb2.y));
 		const float2 sz = f2add(f2(pa1.z, pb1.z), f2(-pa2.z, -pb2.z));
 		const float2 d2g = f2fma(sz, sz, f2fma(sy, sy, f2mul(sx, sx)));
-		const float2 inv_dist = f2(rsqrtf(d2g.x), rsqrtf(d2g.y));
-		float2 r = f2mul(d2g, inv_dist);
-		r.x = d2g.x > 0.0f ? r.x : 0.0f;
-		r.y = d2g.y > 0.0f ? r.y : 0.0f;
-		r = f2mul(r, f2s(L.spacing));
+		// coincident atoms (d2g = 0) get r = 0 from a finite reciprocal
+		const float2 inv_dist = f2(rsqrtf(fmaxf(d2g.x, 1e-30f)), rsqrtf(fmaxf(d2g.y, 1e-30f)));
+		const float2 r = f2mul(f2mul(d2g, inv_dist), f2s(L.spacing));
 		const float2 vbond = f2(Ba.y, Bb.y);          // G for CG-G0 pairs, else 0
 		float2 e = f2mul(vbond, r);
 		float2 pg = vbond;
@@ -349,16 +354,17 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 			const float2 ac = f2(Aa.x, Ab.x), bd = f2(Aa.y, Ab.y);
 			const float2 bd_in = f2mul(bd, in_), ac_im = f2mul(ac, im);
 			const float2 ev = f2add(ac_im, f2neg(bd_in));
-			const bool ca = r.x < 8.0f, cb = r.y < 8.0f;
-			e = f2add(e, f2(ca ? ev.x : 0.0f, cb ? ev.y : 0.0f));
+			// cut-off as a 0/1 factor: the terms are finite for every r (sd >= r - hs)
+			const float2 in8 = f2(lt1(r.x, 8.0f), lt1(r.y, 8.0f));
+			e = f2fma(in8, ev, e);
 			if (GRAD) {
 				const float2 gv = f2mul(f2add(f2mul(fn, bd_in), f2neg(f2mul(fm, ac_im))), inv);
-				pg = f2add(pg, f2(ca ? gv.x : 0.0f, cb ? gv.y : 0.0f));
+				pg = f2fma(in8, gv, pg);
 			}
 		}
 		// electrostatics and desolvation, cut-off 20.48 A
 		{
-			const bool ca = r.x < 20.48f, cb = r.y < 20.48f;
+			const float2 in20 = f2(lt1(r.x, 20.48f), lt1(r.y, 20.48f));
 			float2 inv_r = f2mul(inv_dist, f2s(L.inv_spacing));
 			float2 rr = r;
 			if (rr.x < emd) { rr.x = emd; inv_r.x = inv_emd; }
@@ -373,13 +379,13 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 			const float2 diel = f2fma(f2s(1.10859f), rs2, f2s(0.010358f));
 			const float2 es = f2mul(f2(Ba.x, Bb.x), inv_r);
 			const float2 ee = f2fma(diel, es, desolv);
-			e = f2add(e, f2(ca ? ee.x : 0.0f, cb ? ee.y : 0.0f));
+			e = f2fma(in20, ee, e);
 			if (GRAD) {
 				const float2 t1 = f2mul(f2mul(es, inv_r), diel);
 				const float2 t2 = f2mul(f2mul(f2mul(es, f2s(2.21718f)), rs2), rs);
 				const float2 t3 = f2mul(f2mul(f2s(0.0771605f), rr), desolv);
 				const float2 ge = f2add(f2add(t1, t2), t3);
-				pg = f2add(pg, f2(ca ? -ge.x : 0.0f, cb ? -ge.y : 0.0f));
+				pg = f2fma(f2neg(in20), ge, pg);
 			}
 		}
 		esum = f2add(esum, f2(e.x, has_b ? e.y : 0.0f));
