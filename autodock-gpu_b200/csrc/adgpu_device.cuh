@@ -219,13 +219,14 @@ struct PoseSmem {
 	float4* xyz;
 	int* fx; int* fy; int* fz;
 	float4* tq;
+	float2* gsc;       // sin/cos of theta, phi and half the rotation angle
 	int* gg;
 };
 
 __host__ __device__ inline int pose_smem_bytes(int natoms, int ntors)
 {
 	int n4 = (natoms + 3) & ~3;
-	return (7 * n4) * 4 + ntors * 16 + 64 * 4;
+	return (7 * n4) * 4 + ntors * 16 + 32 + 64 * 4;
 }
 
 __device__ __forceinline__ PoseSmem carve_pose(char* base, int natoms, int ntors)
@@ -235,6 +236,8 @@ __device__ __forceinline__ PoseSmem carve_pose(char* base, int natoms, int ntors
 	float* f = reinterpret_cast<float*>(base);
 	s.tq = reinterpret_cast<float4*>(f);          // 16-byte aligned first
 	f += ntors * 4;
+	s.gsc = reinterpret_cast<float2*>(f);
+	f += 8;
 	s.xyz = reinterpret_cast<float4*>(f);         // still 16-byte aligned
 	f += 4 * n4;
 	s.fx = reinterpret_cast<int*>(f);
@@ -250,19 +253,18 @@ struct GenRot {
 	float sin_theta, sin_half, is_theta_gt_pi;
 };
 
-__device__ __forceinline__ GenRot genrot_of(const float* g, bool has_ligand)
+// The general rotation from the sines and cosines step 1 of score_pose left
+// in shared memory (sin/cos of theta, phi and half the rotation angle,
+// cuda/calcMergeEneGra.cu:92-120).
+__device__ __forceinline__ GenRot genrot_from(const float* g, bool has_ligand, const float2* sc)
 {
 	GenRot r;
 	r.q = make_float4(0.f, 0.f, 0.f, 1.f);
 	r.mv = make_float3(0.f, 0.f, 0.f);
 	r.sin_theta = 0.f; r.sin_half = 0.f; r.is_theta_gt_pi = 1.f;
 	if (has_ligand) {
-		float phi = g[3] * kDegToRad, theta = g[4] * kDegToRad, rotangle = g[5] * kDegToRad;
+		const float st = sc[0].x, ct = sc[0].y, sp = sc[1].x, cp = sc[1].y, sh = sc[2].x, ch = sc[2].y;
 		r.mv = make_float3(g[0], g[1], g[2]);
-		float st, ct, sp, cp, sh, ch;
-		sincosf(theta, &st, &ct);
-		sincosf(phi, &sp, &cp);
-		sincosf(rotangle * 0.5f, &sh, &ch);
 		r.q = make_float4(sh * st * cp, sh * st * sp, sh * ct, ch);
 		r.sin_theta = st; r.sin_half = sh;
 		r.is_theta_gt_pi = 1.0f - 2.0f * (float)(st < 0.0f);
@@ -419,17 +421,28 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
                            const PoseSmem& S, const Group<TPP>& G)
 {
 	const int rank = G.rank;
-	// 1. torsion quaternions (cuda/calcMergeEneGra.cu:160-175, computed once per torsion)
-	for (int k = rank; k < L.ntors; k += TPP) {
+	// 1. torsion quaternions (cuda/calcMergeEneGra.cu:160-175, computed once per
+	//    torsion) and the sines/cosines of the general rotation, one sincos
+	//    per thread: lanes past the torsions take theta, phi and half the angle
+	const bool has_lig = L.nlig > 0;
+	const int nsc = L.ntors + (has_lig ? 3 : 0);
+	for (int k = rank; k < nsc; k += TPP) {
+		const int j = k - L.ntors;
+		const float ang = j < 0 ? g[6 + k] * kDegToRad * 0.5f
+		                        : (j == 0 ? g[4] * kDegToRad : (j == 1 ? g[3] * kDegToRad : g[5] * kDegToRad * 0.5f));
 		float s, c;
-		sincosf(g[6 + k] * kDegToRad * 0.5f, &s, &c);
-		float4 u = L.tors_uv[k];
-		S.tq[k] = make_float4(s * u.x, s * u.y, s * u.z, c);
+		sincosf(ang, &s, &c);
+		if (j < 0) {
+			float4 u = L.tors_uv[k];
+			S.tq[k] = make_float4(s * u.x, s * u.y, s * u.z, c);
+		} else {
+			S.gsc[j] = make_float2(s, c);
+		}
 	}
 	if (GRAD)
 		for (int k = rank; k < L.ngenes; k += TPP) S.gg[k] = 0;
-	const GenRot gr = genrot_of(g, L.nlig > 0);
 	G.sync();
+	const GenRot gr = genrot_from(g, has_lig, S.gsc);
 
 	// 2. pose: each atom applies its own torsion chain, then the general rotation
 	//    (the per-atom order the reference's rotation list encodes, cuda/calcMergeEneGra.cu:131-190);
