@@ -109,6 +109,8 @@ struct TickArgs {
 	int* pending;               // per work item: tasks of the current phase not yet done
 	int* quota;                 // per work item: phases this tick may still run
 	int ga_chunk;               // entities per GA / initial-population task
+	long long tick_ns;          // > 0: runs take no new GA phase once this long after *t0
+	unsigned long long* t0;     // globaltimer at the launch's first worker (host sets ~0)
 	TickClass cls[3];           // threads per pose 32, 64, 128
 };
 
@@ -240,7 +242,10 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 	G.rank = threadIdx.x % TPP;
 	G.bar_id = 1 + local;
 	G.red = nullptr;
-	if (G.rank == 0) { H.req = -1; H.t_enter = global_ns(); H.t_task = 0; H.busy = 0; H.ntask = 0; }
+	if (G.rank == 0) {
+		H.req = -1; H.t_enter = global_ns(); H.t_task = 0; H.busy = 0; H.ntask = 0;
+		if (t.tick_ns > 0) atomicMin(t.t0, (unsigned long long)H.t_enter);
+	}
 	G.sync();
 	for (;;) {
 		if (G.rank == 0) {
@@ -337,7 +342,9 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 			else if (rq.init[run] && ((unsigned long long)rq.evals_runs[run] >= rq.max_evals || rq.gen[run] >= rq.max_gens)) {
 				rq.done[run] = 1;
 				next = kNextBest;
-			} else if (t.quota[w] <= 0) next = kNextRetire;
+			} else if (t.quota[w] <= 0 ||
+			           (t.tick_ns > 0 && global_ns() - (long long)*(volatile unsigned long long*)t.t0 > t.tick_ns))
+				next = kNextRetire;
 			else next = rq.init[run] ? kNextGA : kNextInit;
 			H.next = next;
 			H.cur = rq.cur[run];
@@ -529,7 +536,8 @@ adgpu_status adgpu_engine_create(const adgpu_engine_config* cfg, adgpu_engine** 
 	E.budget = E.cfg.memory_budget_bytes ? E.cfg.memory_budget_bytes : (size_t)(0.8 * fr);
 	e = cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking);
 	if (e != cudaSuccess) { delete en; return cuda_fail(e, "stream"); }
-	e = cudaMalloc(&E.d_ctl, 12 * sizeof(QueueCtl));
+	if (E.cfg.tick_ms < 0.0f || E.cfg.tick_ms != E.cfg.tick_ms) { delete en; return fail(ADGPU_ERR_ARG, "tick_ms must be >= 0"); }
+	e = cudaMalloc(&E.d_ctl, 12 * sizeof(QueueCtl) + sizeof(unsigned long long));
 	if (e != cudaSuccess) { delete en; return cuda_fail(e, "engine queues"); }
 	*out = en;
 	return ADGPU_OK;
@@ -747,6 +755,8 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 		memset(&t, 0, sizeof(t));
 		t.reqs = E.d_reqs; t.work = E.d_work; t.work_done = E.d_done;
 		t.pending = E.d_pending; t.quota = E.d_quota; t.ga_chunk = chunk;
+		t.tick_ns = (long long)(1e6 * (double)E.cfg.tick_ms);
+		t.t0 = reinterpret_cast<unsigned long long*>(E.d_ctl + 12);     // this launch's start, set by its workers
 		for (int k = 0; k < 3; k++) {
 			const int c = k * 4 + m;
 			nr[k] = (int)work[c].size(); ma[k] = max_atoms[c]; mt[k] = max_tors[c]; mx[k] = max_tasks[c]; wt[k] = weight[c];
@@ -756,6 +766,10 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 			any |= nr[k] > 0;
 		}
 		if (!any) continue;
+		if (t.tick_ns > 0) {
+			e = cudaMemsetAsync(t.t0, 0xFF, sizeof(unsigned long long), E.stream);     // ~0: no worker yet
+			if (e != cudaSuccess) return cuda_fail(e, "tick start");
+		}
 		adgpu_status st = ADGPU_OK;
 		switch (m) {
 		case LS_SW: st = launch_engine<LS_SW>(E, t, nr, wt, mx, ma, mt); break;

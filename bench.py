@@ -395,17 +395,29 @@ def run_batch(args):
     runs admitted at once, one persistent launch) next to plain
     per-ligand dockings through the reference kernel API, same ligands, same
     budget.  A bounded sample of the batching configuration (1024 ligands,
-    10-64 heavy atoms, 0-32 torsions, nrun 20, 2.5M evals per run)."""
+    10-64 heavy atoms, 0-32 torsions, nrun 20, 2.5M evals per run), or with
+    --batch-config 4 of the flexible-receptor one (80^3 maps, 7 types + e + d,
+    2 flexible residues of 8-10 atoms and 2-4 torsions, nrun 50, ADAM)."""
     import torch
     from adgpu_b200 import device, dock, engine, frontend, synth
     w = WORKLOAD
-    spec = synth.grid_spec(w["npts"], w["types"], seed=12345 + 3)
-    grid = frontend.Grid.from_maps(synth.quantize_maps(synth.make_maps_fast(spec)), w["types"], spec.spacing, spec.origin)
+    cfg4 = getattr(args, "batch_config", 3) == 4
+    types = synth.MAP_TYPES_7 if cfg4 else w["types"]
+    spec = synth.grid_spec(80 if cfg4 else w["npts"], types, seed=12345 + (4 if cfg4 else 3))
+    grid = frontend.Grid.from_maps(synth.quantize_maps(synth.make_maps_fast(spec)), types, spec.spacing, spec.origin)
     rng = np.random.default_rng(3)
-    nlig, nrun, nev = args.nlig, 20, args.nev
+    nlig, nrun, nev = args.nlig, (50 if cfg4 else 20), args.nev
     sizes = [(int(rng.integers(10, 65)), int(rng.integers(0, 33))) for _ in range(nlig)]
     run = frontend.default_dockpars(grid.spacing, 150)
-    ligs = [frontend.Ligand(grid, _ligand_text(3, i, a, t), None, run=run, seed=w["seed"], num_runs=nrun)
+    flex = None
+    ltypes = None
+    if cfg4:
+        frng = np.random.default_rng(77)
+        flex = synth.flexres_text([synth.make_flexres(100 + k, int(frng.integers(8, 11)), int(frng.integers(2, 5)),
+                                                      anchor=np.array([-3.0 + 6.0 * k, 4.0, 0.0])) for k in range(2)])
+        ltypes = (("C", 0.55), ("A", 0.15), ("N", 0.08), ("NA", 0.04), ("OA", 0.13), ("SA", 0.05))
+    ligs = [frontend.Ligand(grid, _ligand_text(4 if cfg4 else 3, i, a, t, types=ltypes), flex, run=run,
+                            seed=w["seed"], num_runs=nrun)
             for i, (a, t) in enumerate(sizes)]
     # batched: one engine, everything admitted, run to completion
     en = engine.Engine(threads_per_pose=args.engine_tpp)
@@ -449,7 +461,8 @@ def run_batch(args):
         plain[name] = {"ligands_sampled": nplain, "seconds": t_plain, "ligands_per_hour": 3600.0 * nplain / t_plain / scale,
                        "evals_per_s": ev_plain / t_plain, "sample_cost_scale": scale}
     lph_b = 3600.0 * nlig / t_batch
-    return {"mode": "batch", "ligands": nlig, "nrun": nrun, "nev_per_run": nev, "lsmet": args.lsmet,
+    return {"mode": "batch", "config": 4 if cfg4 else 3, "flexres": 2 if cfg4 else 0,
+            "ligands": nlig, "nrun": nrun, "nev_per_run": nev, "lsmet": args.lsmet,
             "heavy_atoms": [min(a for a, _ in sizes), max(a for a, _ in sizes)],
             "batched": {"seconds": t_batch, "ligands_per_hour": lph_b, "evals_per_s": ev_batch / t_batch,
                         "worker_utilisation": util, "tasks": int(st.tasks)},
@@ -480,18 +493,22 @@ def run_serve(args):
     ligs = [frontend.Ligand(grids[t], texts[i], None, run=frontend.default_dockpars(grids[t].spacing, 150),
                             seed=w["seed"], num_runs=nrun) for i, t in enumerate(targets)]
     budget = args.budget_gb << 30
-    # capacity: a batch of requests run to completion
+    # capacity: a batch of requests run to completion in one launch
     cap_n = min(nreq, 48)
-    en = engine.Engine(memory_budget_bytes=budget, gens_per_tick=4)
-    recs = [en.add_receptor(g) for g in grids]
+    cap = engine.Engine(memory_budget_bytes=budget)
+    crecs = [cap.add_receptor(g) for g in grids]
     t0 = time.perf_counter()
-    ids = [en.submit(ligs[i], recs[targets[i]], args.lsmet, max_evals=nev) for i in range(cap_n)]
-    en.run()
+    ids = [cap.submit(ligs[i], crecs[targets[i]], args.lsmet, max_evals=nev) for i in range(cap_n)]
+    cap.run()
     for i in ids:
-        en.result(i)
+        cap.result(i)
     capacity = cap_n / (time.perf_counter() - t0)          # ligands / s
+    cap.close()
     rate = 0.8 * capacity
     arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    # the serving engine: ticks end on a wall-clock deadline (or a generation count)
+    en = engine.Engine(memory_budget_bytes=budget, gens_per_tick=args.gens_per_tick, tick_ms=args.tick_ms)
+    recs = [en.add_receptor(g) for g in grids]
     # serving loop
     t_start = time.perf_counter()
     pending, live, lat, queued = list(range(nreq)), {}, [], []
@@ -522,7 +539,10 @@ def run_serve(args):
     return {"mode": "serve", "requests": nreq, "nrun": nrun, "nev_per_run": nev, "receptors": "60^3, 80^3, 100^3",
             "batched_capacity_ligands_per_s": capacity, "arrival_rate_per_s": rate,
             "ligands_per_hour": 3600.0 * nreq / t_total, "latency_p50_s": float(np.percentile(lat, 50)),
-            "latency_p99_s": float(np.percentile(lat, 99)), "memory_budget_gb": args.budget_gb}
+            "latency_p99_s": float(np.percentile(lat, 99)), "memory_budget_gb": args.budget_gb,
+            "gens_per_tick": args.gens_per_tick, "tick_ms": args.tick_ms, "ticks": int(en.stats().ticks),
+            "worker_utilisation": (en.stats().worker_busy_s / en.stats().worker_span_s
+                                   if en.stats().worker_span_s > 0 else None)}
 
 
 def _hbm_peak():
@@ -547,10 +567,14 @@ def main():
     ap.add_argument("--engine-tpp", type=int, default=0,
                     help="engine threads per pose (batch mode): 0 = autotuned per ligand size, or 32, 64, 128")
     ap.add_argument("--nlig", type=int, default=64, help="ligands (batch mode)")
+    ap.add_argument("--batch-config", type=int, default=3, choices=[3, 4],
+                    help="batch mode workload: 3 (uneven ligands) or 4 (80^3 maps, 2 flexible residues, nrun 50)")
     ap.add_argument("--nev", type=int, default=250_000, help="evaluations per run (batch / serve modes)")
     ap.add_argument("--plain-sample", type=int, default=16, help="ligands docked one at a time for the plain arm")
     ap.add_argument("--nreq", type=int, default=200, help="requests (serve mode)")
     ap.add_argument("--budget-gb", type=int, default=8, help="engine device-memory budget (serve mode)")
+    ap.add_argument("--gens-per-tick", type=int, default=0, help="generations per engine tick (serve mode; 0: no limit)")
+    ap.add_argument("--tick-ms", type=float, default=50.0, help="wall-clock length of an engine tick (serve mode; 0: none)")
     args = ap.parse_args()
     if args.mode == "ls-kernel":
         run_kernel_only(args)

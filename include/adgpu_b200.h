@@ -337,12 +337,13 @@ adgpu_status adgpu_ligand_population(const adgpu_ligand* lig, float* initpop, si
  * Receptor maps stay resident; each submitted request (a prepared ligand
  * with its runs) keeps its populations, energies, eval counters and PRNG
  * states on the device until its result is taken.  adgpu_engine_tick
- * advances every admitted run by up to gens_per_tick generations in one
- * persistent launch per threads-per-pose class (a CTA carries a run through
- * whole generations: GA, local search, eval sum, stop test); between ticks
- * requests can be submitted and results taken (continuous batching).  Each
- * run stops on its own budget (evals >= max_evals or generations >=
- * max_gens), so a request's result does not depend on what else is running.
+ * advances every admitted run by up to gens_per_tick generations, or until
+ * tick_ms has passed, in one persistent launch per local-search method whose
+ * pose groups take tasks (GA chunks, single local searches) from device
+ * queues; between ticks requests can be submitted and results taken
+ * (continuous batching).  Each run stops on its own budget (evals >=
+ * max_evals or generations >= max_gens), so a request's result does not
+ * depend on what else is running or on where ticks end.
  * ------------------------------------------------------------------------- */
 typedef struct adgpu_engine_s adgpu_engine;
 
@@ -351,6 +352,7 @@ typedef struct {
 	int    threads_per_pose;     /* 32, 64 or 128; 0: tuned per ligand size class */
 	int    gens_per_tick;        /* generations per tick; <= 0: run every admitted run to completion */
 	int    device;               /* CUDA device ordinal */
+	float  tick_ms;              /* > 0: a tick also ends after this long: runs take no new GA phase after it */
 } adgpu_engine_config;
 
 typedef struct {

@@ -159,3 +159,32 @@ def test_ga_only_and_mixed_population_sizes(grid, monkeypatch):
         assert r.best_energies[0] == best
         if rate == 0.0:
             assert int(r.evals[0]) == pop * (gens + 1) - gens    # GA only: P per generation minus the elite
+
+
+def test_time_sliced_ticks_give_the_same_results(grid):
+    """Ticks that end on a wall-clock deadline (tick_ms) instead of a
+    generation count cut runs at arbitrary generations; results must not
+    depend on where the cuts fall."""
+    ligs = [ligand(grid, 30 + i, 16 + 4 * i, 3 + i, runs=2) for i in range(3)]
+    nev = 30_000
+    ref = []
+    for lg in ligs:
+        en = engine.Engine(threads_per_pose=32)
+        rec = en.add_receptor(grid)
+        rid = en.submit(lg, rec, "ad", max_evals=nev)
+        en.run()
+        ref.append(en.result(rid))
+        en.close()
+    en = engine.Engine(threads_per_pose=32, tick_ms=2.0)
+    rec = en.add_receptor(grid)
+    ids = [en.submit(lg, rec, "ad", max_evals=nev) for lg in ligs]
+    ticks = 0
+    while not all(en.done(r) for r in ids):
+        en.tick()
+        ticks += 1
+        assert ticks < 100000
+    assert ticks > 1
+    for rid, r0 in zip(ids, ref):
+        r = en.result(rid)
+        np.testing.assert_array_equal(r.best_energies, r0.best_energies)
+        np.testing.assert_array_equal(r.evals, r0.evals)
