@@ -24,7 +24,8 @@ class RequestParams(C.Structure):
 class EngineStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("ticks", C.c_uint64),
                 ("bytes_used", C.c_size_t), ("bytes_budget", C.c_size_t), ("active", C.c_int),
-                ("worker_busy_s", C.c_double), ("worker_span_s", C.c_double), ("tasks", C.c_uint64)]
+                ("worker_busy_s", C.c_double), ("worker_span_s", C.c_double), ("tasks", C.c_uint64),
+                ("kernel_s", C.c_double)]
 
 
 _vp = C.c_void_p

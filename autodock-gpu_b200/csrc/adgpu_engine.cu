@@ -39,6 +39,7 @@ struct ReqDev {
 	float* conf[2];             // R*P*64, double buffered
 	float* e[2];                // R*P
 	int* evals_runs;            // R
+	int* pending;               // R tasks of the run's current phase not yet done
 	uint32_t* gen;              // R generations done
 	uint8_t* cur;               // R current buffer index
 	uint8_t* done;              // R run finished
@@ -106,11 +107,9 @@ struct TickArgs {
 	const ReqDev* reqs;
 	const RunRef* work;
 	uint8_t* work_done;         // per work item: run finished (written when it retires)
-	int* pending;               // per work item: tasks of the current phase not yet done
 	int* quota;                 // per work item: phases this tick may still run
 	int ga_chunk;               // entities per GA / initial-population task
-	long long tick_ns;          // > 0: runs take no new GA phase once this long after *t0
-	unsigned long long* t0;     // globaltimer at the launch's first worker (host sets ~0)
+	long long tick_ns;          // > 0: a worker takes no new task once this long after it started
 	TickClass cls[3];           // threads per pose 32, 64, 128
 };
 
@@ -119,6 +118,7 @@ struct GroupHdr {
 	KArgs a;                    // the current request's arguments, pointers set per task
 	unsigned long long pos;
 	long long t_enter, t_task;           // worker accounting (rank 0 only)
+	long long deadline;                  // globaltimer after which no task is taken; 0: none
 	unsigned long long busy, ntask;
 	int task, last, req, next, cur, isum;
 	float bv[4];
@@ -134,13 +134,15 @@ __device__ __forceinline__ long long global_ns()
 }
 
 // Next task of a class, or -1 when the worker should stop: every run of the
-// class has retired, the queue stayed empty for kIdleNs, or (error) a
-// reserved slot was never written.
-__device__ int queue_pop(const TickClass& C)
+// class has retired, the tick's time is up (tasks still queued stay for the
+// next tick), the queue stayed empty for kIdleNs, or (error) a reserved slot
+// was never written.
+__device__ int queue_pop(const TickClass& C, long long deadline)
 {
 	volatile QueueCtl* vq = C.ctl;
 	long long idle_since = -1;
 	for (int spins = 0; spins < (1 << 28); spins++) {
+		if (deadline && global_ns() > deadline) return -1;
 		const unsigned long long h = vq->head, t = vq->tail;
 		if (h < t) {
 			if (atomicCAS(&C.ctl->head, h, h + 1) != h) continue;
@@ -244,13 +246,13 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 	G.red = nullptr;
 	if (G.rank == 0) {
 		H.req = -1; H.t_enter = global_ns(); H.t_task = 0; H.busy = 0; H.ntask = 0;
-		if (t.tick_ns > 0) atomicMin(t.t0, (unsigned long long)H.t_enter);
+		H.deadline = t.tick_ns > 0 ? H.t_enter + t.tick_ns : 0;
 	}
 	G.sync();
 	for (;;) {
 		if (G.rank == 0) {
 			if (H.t_task) H.busy += (unsigned long long)(global_ns() - H.t_task);
-			H.task = queue_pop(C);
+			H.task = queue_pop(C, H.deadline);
 			H.t_task = H.task >= 0 ? global_ns() : 0;
 			H.ntask += H.task >= 0;
 		}
@@ -309,14 +311,14 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 			// the last task of the phase goes on to finalise it
 			__threadfence();
 			G.sync();
-			if (G.rank == 0) H.last = (atomicSub(&t.pending[w], 1) == 1);
+			if (G.rank == 0) H.last = (atomicSub(&rq.pending[run], 1) == 1);
 			G.sync();
 			if (!H.last) continue;
 			__threadfence();
 		}
 		// ---- phase end ----
 		if (kind == kTaskGA && L > 0 && a.dp.lsearch_rate != 0.0f) {
-			if (G.rank == 0) { t.pending[w] = L; __threadfence(); }
+			if (G.rank == 0) { rq.pending[run] = L; __threadfence(); }
 			G.sync();
 			queue_push<TPP>(C, w, kTaskLS, L, G, H);
 			continue;
@@ -342,8 +344,7 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 			else if (rq.init[run] && ((unsigned long long)rq.evals_runs[run] >= rq.max_evals || rq.gen[run] >= rq.max_gens)) {
 				rq.done[run] = 1;
 				next = kNextBest;
-			} else if (t.quota[w] <= 0 ||
-			           (t.tick_ns > 0 && global_ns() - (long long)*(volatile unsigned long long*)t.t0 > t.tick_ns))
+			} else if (t.quota[w] <= 0 || (H.deadline && global_ns() > H.deadline))
 				next = kNextRetire;
 			else next = rq.init[run] ? kNextGA : kNextInit;
 			H.next = next;
@@ -353,7 +354,7 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 		const int next = H.next;
 		if (next == kNextGA || next == kNextInit) {
 			const int nch = (P + t.ga_chunk - 1) / t.ga_chunk;
-			if (G.rank == 0) { t.pending[w] = nch; __threadfence(); }
+			if (G.rank == 0) { rq.pending[run] = nch; __threadfence(); }
 			G.sync();
 			queue_push<TPP>(C, w, next == kNextGA ? kTaskGA : kTaskInit, nch, G, H);
 			continue;
@@ -408,6 +409,9 @@ struct Request {
 	bool done = false;
 	int natoms = 0, ntors = 0;
 	double t_submit = 0, t_done = 0;
+	// per run: tasks (kind | index bits of the task word) still queued when a
+	// tick's time ran out; they open the run's part of the next tick
+	std::vector<std::vector<uint32_t>> leftover;
 };
 
 static double now_s()
@@ -434,18 +438,26 @@ struct Engine {
 	unsigned long long* d_slots = nullptr; size_t d_slots_cap = 0;
 	QueueCtl* d_ctl = nullptr;
 	int ga_chunk = 16;
+	cudaMemPool_t pool = nullptr;                 // request tables and state, kept by the pool when freed
+	cudaEvent_t ev0 = nullptr, ev1 = nullptr;     // around a tick's launches
 	std::vector<uint8_t> h_done;
 	std::map<long, int> tpp_cache;     // size bucket -> tuned threads per pose
 	adgpu_engine_stats stats{};
 	std::mutex mu;
 	~Engine()
 	{
+		for (auto& kv : requests)
+			if (kv.second->state) { cudaFreeAsync(kv.second->state, stream); kv.second->state = nullptr; }
+		if (stream) cudaStreamSynchronize(stream);
 		requests.clear();
 		receptors.clear();
+		if (pool) cudaMemPoolDestroy(pool);
 		if (d_reqs) cudaFree(d_reqs);
 		if (d_work) cudaFree(d_work);
 		if (d_slots) cudaFree(d_slots);
 		if (d_ctl) cudaFree(d_ctl);
+		if (ev0) cudaEventDestroy(ev0);
+		if (ev1) cudaEventDestroy(ev1);
 		if (stream) cudaStreamDestroy(stream);
 	}
 };
@@ -454,7 +466,7 @@ static size_t request_bytes(int runs, int pop, size_t tables)
 {
 	size_t n = (size_t)runs * pop;
 	return tables + n * kGenotypeStride * 4 * 3 /* conf x2, prng */ + n * 4 * 3 /* e x2, evals_new */ +
-	       (size_t)runs * (4 + 4 + 3 + 4 + kGenotypeStride * 4) + 1024;
+	       (size_t)runs * (4 + 4 + 4 + 3 + 4 + kGenotypeStride * 4) + 1024;
 }
 
 // Launches the tick's kernel for local search LSMET.  Its CTAs are split
@@ -537,7 +549,17 @@ adgpu_status adgpu_engine_create(const adgpu_engine_config* cfg, adgpu_engine** 
 	e = cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking);
 	if (e != cudaSuccess) { delete en; return cuda_fail(e, "stream"); }
 	if (E.cfg.tick_ms < 0.0f || E.cfg.tick_ms != E.cfg.tick_ms) { delete en; return fail(ADGPU_ERR_ARG, "tick_ms must be >= 0"); }
-	e = cudaMalloc(&E.d_ctl, 12 * sizeof(QueueCtl) + sizeof(unsigned long long));
+	{
+		cudaMemPoolProps props{};
+		props.allocType = cudaMemAllocationTypePinned;
+		props.location.type = cudaMemLocationTypeDevice;
+		props.location.id = E.cfg.device;
+		e = cudaMemPoolCreate(&E.pool, &props);
+		if (e != cudaSuccess) { delete en; return cuda_fail(e, "engine memory pool"); }
+		uint64_t keep = ~0ull;          // freed request memory stays in the pool for the next admission
+		cudaMemPoolSetAttribute(E.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+	}
+	e = cudaMalloc(&E.d_ctl, 12 * sizeof(QueueCtl));
 	if (e != cudaSuccess) { delete en; return cuda_fail(e, "engine queues"); }
 	*out = en;
 	return ADGPU_OK;
@@ -597,27 +619,29 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 	if (st != ADGPU_OK) return st;
 	const size_t need = request_bytes(runs, dp.pop_size, pk.blob.size());
 	if (E.used + need > E.budget) return fail(ADGPU_ERR_BUDGET, "request does not fit the engine's memory budget now");
-	st = upload_ligand(pk, r->tables);
-	if (st != ADGPU_OK) return st;
-	set_grid_fields(r->tables.dev, dp, R.cells);
-	r->tables.own_grid = false;
-	r->tables.dgrid = nullptr;
-	// one allocation for the request's state
+	// one stream-ordered allocation from the engine's pool for the request's
+	// tables and state (no device-wide synchronisation on admit or release)
 	const size_t n = (size_t)runs * dp.pop_size;
 	size_t off = 0;
 	auto take = [&](size_t bytes) { size_t o = off; off = (off + bytes + 255) / 256 * 256; return o; };
-	size_t o_c0 = take(n * kGenotypeStride * 4), o_c1 = take(n * kGenotypeStride * 4), o_e0 = take(n * 4),
+	size_t o_tab = take(pk.blob.size()), o_c0 = take(n * kGenotypeStride * 4), o_c1 = take(n * kGenotypeStride * 4), o_e0 = take(n * 4),
 	       o_e1 = take(n * 4), o_ev = take(n * 4), o_pr = take(n * 64 * 4), o_er = take(runs * 4), o_gen = take(runs * 4),
 	       o_cur = take(runs), o_done = take(runs), o_init = take(runs), o_be = take(runs * 4),
-	       o_bg = take((size_t)runs * kGenotypeStride * 4);
-	cudaError_t e = cudaMalloc(&r->state, off);
+	       o_bg = take((size_t)runs * kGenotypeStride * 4), o_pend = take((size_t)runs * 4);
+	cudaError_t e = cudaMallocFromPoolAsync(&r->state, off, E.pool, E.stream);
 	if (e != cudaSuccess) return cuda_fail(e, "request state");
 	char* B = static_cast<char*>(r->state);
-	e = cudaMemsetAsync(B, 0, off, E.stream);
+	e = cudaMemsetAsync(B + o_c0, 0, off - o_c0, E.stream);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(B + o_tab, pk.blob.data(), pk.blob.size(), cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(B + o_c0, p.initpop.data(), n * kGenotypeStride * 4, cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(B + o_pr, p.prng.data(), n * 64 * 4, cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
-	if (e != cudaSuccess) { cudaFree(r->state); r->state = nullptr; return cuda_fail(e, "request upload"); }
+	if (e != cudaSuccess) { cudaFreeAsync(r->state, E.stream); r->state = nullptr; return cuda_fail(e, "request upload"); }
+	place_ligand(pk, B + o_tab, r->tables.dev);
+	set_grid_fields(r->tables.dev, dp, R.cells);
+	r->tables.own_grid = false;
+	r->tables.dgrid = nullptr;
+	r->tables.packed = pk;
 	ReqDev& d = r->dev;
 	memset(&d, 0, sizeof(d));
 	d.a.L = r->tables.dev;
@@ -636,6 +660,7 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 	d.init = reinterpret_cast<uint8_t*>(B + o_init);
 	d.best_e = reinterpret_cast<float*>(B + o_be);
 	d.best_g = reinterpret_cast<float*>(B + o_bg);
+	d.pending = reinterpret_cast<int*>(B + o_pend);
 	d.max_evals = rp->max_evals;
 	d.max_gens = rp->max_gens ? rp->max_gens : 0xFFFFFFFFu;
 	d.lsmet = rp->lsmet;
@@ -643,6 +668,7 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 	r->id = E.next_id++;
 	r->receptor = rp->receptor;
 	r->runs = runs;
+	r->leftover.assign(runs, {});
 	r->bytes = need;
 	r->natoms = dp.num_of_atoms;
 	r->ntors = dp.num_of_genes - 6;
@@ -723,16 +749,25 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 		e = cudaMalloc(&E.d_slots, E.d_slots_cap * sizeof(unsigned long long));
 		if (e != cudaSuccess) { E.d_slots = nullptr; E.d_slots_cap = 0; return cuda_fail(e, "task rings"); }
 	}
-	// initial state: every run's START task queued in its class's ring (lap 1),
-	// the rest of the ring empty (lap 0 matches no position)
-	std::vector<unsigned long long> h_start(nwork);
+	// initial state, queued in each class's ring (lap 1; the rest of the ring
+	// empty, lap 0 matches no position): the tasks a run had still queued when
+	// the previous tick's time ran out, else its START task
+	std::vector<unsigned long long> h_init[NC];
 	std::vector<int> h_quota(nwork, E.cfg.gens_per_tick);
 	QueueCtl h_ctl[NC];
 	memset(h_ctl, 0, sizeof(h_ctl));
 	for (int c = 0; c < NC; c++) {
-		for (size_t i = 0; i < work[c].size(); i++)
-			h_start[start[c] + i] = (1ull << 32) | task_word((uint32_t)(start[c] + i), kTaskStart, 0);
-		h_ctl[c].tail = work[c].size();
+		for (size_t i = 0; i < work[c].size(); i++) {
+			const uint32_t w = (uint32_t)(start[c] + i);
+			std::vector<uint32_t>& left = order[work[c][i].req]->leftover[work[c][i].run];
+			if (left.empty()) {
+				h_init[c].push_back((1ull << 32) | task_word(w, kTaskStart, 0));
+			} else {
+				for (uint32_t kind_idx : left) h_init[c].push_back((1ull << 32) | (w << (kTaskIdxBits + 2)) | kind_idx);
+				left.clear();
+			}
+		}
+		h_ctl[c].tail = h_init[c].size();
 		h_ctl[c].alive = (int)work[c].size();
 		h_ctl[c].t_first = ~0ull;
 	}
@@ -742,11 +777,13 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	if (e == cudaSuccess) e = cudaMemsetAsync(E.d_done, 0, nwork, E.stream);
 	if (e == cudaSuccess) e = cudaMemsetAsync(E.d_slots, 0, slots * sizeof(unsigned long long), E.stream);
 	for (int c = 0; c < NC && e == cudaSuccess; c++)
-		if (!work[c].empty())
-			e = cudaMemcpyAsync(E.d_slots + slot0[c], h_start.data() + start[c], work[c].size() * sizeof(unsigned long long),
+		if (!h_init[c].empty())
+			e = cudaMemcpyAsync(E.d_slots + slot0[c], h_init[c].data(), h_init[c].size() * sizeof(unsigned long long),
 			                    cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_ctl, h_ctl, sizeof(h_ctl), cudaMemcpyHostToDevice, E.stream);
 	if (e != cudaSuccess) return cuda_fail(e, "tick upload");
+	if (!E.ev0) { cudaEventCreate(&E.ev0); cudaEventCreate(&E.ev1); }
+	cudaEventRecord(E.ev0, E.stream);
 	for (int m = 0; m < 4; m++) {
 		int nr[3], ma[3], mt[3], mx[3];
 		double wt[3];
@@ -754,9 +791,8 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 		TickArgs t;
 		memset(&t, 0, sizeof(t));
 		t.reqs = E.d_reqs; t.work = E.d_work; t.work_done = E.d_done;
-		t.pending = E.d_pending; t.quota = E.d_quota; t.ga_chunk = chunk;
+		t.quota = E.d_quota; t.ga_chunk = chunk;
 		t.tick_ns = (long long)(1e6 * (double)E.cfg.tick_ms);
-		t.t0 = reinterpret_cast<unsigned long long*>(E.d_ctl + 12);     // this launch's start, set by its workers
 		for (int k = 0; k < 3; k++) {
 			const int c = k * 4 + m;
 			nr[k] = (int)work[c].size(); ma[k] = max_atoms[c]; mt[k] = max_tors[c]; mx[k] = max_tasks[c]; wt[k] = weight[c];
@@ -766,10 +802,6 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 			any |= nr[k] > 0;
 		}
 		if (!any) continue;
-		if (t.tick_ns > 0) {
-			e = cudaMemsetAsync(t.t0, 0xFF, sizeof(unsigned long long), E.stream);     // ~0: no worker yet
-			if (e != cudaSuccess) return cuda_fail(e, "tick start");
-		}
 		adgpu_status st = ADGPU_OK;
 		switch (m) {
 		case LS_SW: st = launch_engine<LS_SW>(E, t, nr, wt, mx, ma, mt); break;
@@ -779,20 +811,42 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 		}
 		if (st != ADGPU_OK) return st;
 	}
+	cudaEventRecord(E.ev1, E.stream);
 	E.h_done.resize(nwork);
 	e = cudaMemcpyAsync(E.h_done.data(), E.d_done, nwork, cudaMemcpyDeviceToHost, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(h_ctl, E.d_ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, E.stream);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
 	if (e != cudaSuccess) return cuda_fail(e, "engine tick");
+	const bool timed = E.cfg.tick_ms > 0.0f;
 	for (int c = 0; c < NC; c++) {
 		if (h_ctl[c].err) return fail(ADGPU_ERR_TIMEOUT, "engine task queue: a reserved slot was never written");
-		if (h_ctl[c].alive != 0) return fail(ADGPU_ERR_STATE, "engine tick ended with runs still active");
+		if (h_ctl[c].alive != 0 && !timed) return fail(ADGPU_ERR_STATE, "engine tick ended with runs still active");
+		// tasks left queued when the tick's time ran out go back to their runs
+		if (timed && h_ctl[c].tail > h_ctl[c].head) {
+			const unsigned long long h = h_ctl[c].head, n = h_ctl[c].tail - h;
+			if (n > cap[c]) return fail(ADGPU_ERR_STATE, "engine task ring overran");
+			std::vector<unsigned long long> left(n);
+			const unsigned long long first = std::min<unsigned long long>(n, cap[c] - h % cap[c]);
+			e = cudaMemcpy(left.data(), E.d_slots + slot0[c] + h % cap[c], first * 8, cudaMemcpyDeviceToHost);
+			if (e == cudaSuccess && n > first)
+				e = cudaMemcpy(left.data() + first, E.d_slots + slot0[c], (n - first) * 8, cudaMemcpyDeviceToHost);
+			if (e != cudaSuccess) return cuda_fail(e, "queued tasks");
+			for (unsigned long long k = 0; k < n; k++) {
+				const uint64_t v = left[k];
+				if ((v >> 32) != (h + k) / cap[c] + 1) return fail(ADGPU_ERR_STATE, "engine task ring: unwritten slot after the tick");
+				const uint32_t tw = (uint32_t)v, w = tw >> (kTaskIdxBits + 2);
+				if (w >= nwork) return fail(ADGPU_ERR_STATE, "engine task ring: bad run index");
+				order[all[w].req]->leftover[all[w].run].push_back(tw & ((1u << (kTaskIdxBits + 2)) - 1));
+			}
+		}
 		if (h_ctl[c].workers > 0 && h_ctl[c].t_last > h_ctl[c].t_first) {
 			E.stats.worker_busy_s += 1e-9 * (double)h_ctl[c].busy_ns;
 			E.stats.worker_span_s += 1e-9 * (double)h_ctl[c].workers * (double)(h_ctl[c].t_last - h_ctl[c].t_first);
 			E.stats.tasks += h_ctl[c].tasks;
 		}
 	}
+	float kms = 0.0f;
+	if (cudaEventElapsedTime(&kms, E.ev0, E.ev1) == cudaSuccess) E.stats.kernel_s += 1e-3 * kms;
 	E.stats.ticks++;
 	// a request is complete when all its runs are
 	std::vector<int> runs_done(order.size(), 0);
@@ -856,7 +910,7 @@ adgpu_status adgpu_engine_result(adgpu_engine* en, uint64_t request_id, float* b
 	if (e != cudaSuccess) return cuda_fail(e, "result download");
 	if (latency_s) *latency_s = r.t_done - r.t_submit;
 	// release the request's device memory: its slots are free for new admissions
-	if (r.state) cudaFree(r.state);
+	if (r.state) cudaFreeAsync(r.state, E.stream);
 	r.state = nullptr;
 	E.used -= r.bytes;
 	E.requests.erase(it);

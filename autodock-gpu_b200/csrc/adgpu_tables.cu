@@ -160,8 +160,14 @@ adgpu_status upload_ligand(const PackedLigand& p, LigandTables& t)
 	}
 	cudaError_t e = cudaMemcpy(t.dmem, p.blob.data(), p.blob.size(), cudaMemcpyHostToDevice);
 	if (e != cudaSuccess) return cuda_fail(e, "ligand tables upload");
-	const uint8_t* D = static_cast<const uint8_t*>(t.dmem);
-	LigDev& L = t.dev;
+	place_ligand(p, t.dmem, t.dev);
+	t.packed = p;
+	return ADGPU_OK;
+}
+
+void place_ligand(const PackedLigand& p, const void* dbase, LigDev& L)
+{
+	const uint8_t* D = static_cast<const uint8_t*>(dbase);
 	L.natoms = p.natoms; L.nlig = p.nlig; L.ngenes = p.ngenes; L.ntors = p.ntors; L.npairs = p.npairs; L.ntoritems = p.ntoritems;
 	L.atom_xyzq = reinterpret_cast<const float4*>(D + p.off_atom_xyzq);
 	L.atom_info = reinterpret_cast<const uint32_t*>(D + p.off_atom_info);
@@ -172,8 +178,6 @@ adgpu_status upload_ligand(const PackedLigand& p, LigandTables& t)
 	L.tors_ends = reinterpret_cast<const int2*>(D + p.off_tors_ends);
 	L.tor_items = reinterpret_cast<const uint32_t*>(D + p.off_tor_items);
 	L.pairs = reinterpret_cast<const PairRec*>(D + p.off_pairs);
-	t.packed = p;
-	return ADGPU_OK;
 }
 
 void set_grid_fields(LigDev& L, const adgpu_dockpars& dp, const float* cell_grid)

@@ -48,6 +48,8 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 
 // Uploads a packed ligand (tables only; grid pointers left unset).
 adgpu_status upload_ligand(const PackedLigand& p, LigandTables& t);
+// LigDev table pointers for a packed blob already copied to device address dbase.
+void place_ligand(const PackedLigand& p, const void* dbase, LigDev& L);
 
 // Fills the grid fields of a LigDev from the dockpars and a cell-record grid.
 void set_grid_fields(LigDev& L, const adgpu_dockpars& dp, const float* cell_grid);

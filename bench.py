@@ -504,7 +504,7 @@ def run_serve(args):
         cap.result(i)
     capacity = cap_n / (time.perf_counter() - t0)          # ligands / s
     cap.close()
-    rate = 0.8 * capacity
+    rate = args.rate if args.rate > 0 else 0.8 * capacity
     arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
     # the serving engine: ticks end on a wall-clock deadline (or a generation count)
     en = engine.Engine(memory_budget_bytes=budget, gens_per_tick=args.gens_per_tick, tick_ms=args.tick_ms)
@@ -513,10 +513,12 @@ def run_serve(args):
     t_start = time.perf_counter()
     pending, live, lat, queued = list(range(nreq)), {}, [], []
     done_n = 0
+    t_submit = t_tick = t_result = 0.0
     while done_n < nreq:
         now = time.perf_counter() - t_start
         while pending and arrivals[pending[0]] <= now:
             queued.append(pending.pop(0))
+        ta = time.perf_counter()
         while queued:
             i = queued[0]
             rid = en.submit(ligs[i], recs[targets[i]], args.lsmet, max_evals=nev, raise_on_budget=False)
@@ -524,13 +526,18 @@ def run_serve(args):
                 break
             live[rid] = i
             queued.pop(0)
+        tb = time.perf_counter()
+        t_submit += tb - ta
         if live:
             en.tick()
+            tc = time.perf_counter()
+            t_tick += tc - tb
             for rid in [r for r in live if en.done(r)]:
                 i = live.pop(rid)
                 en.result(rid)
                 lat.append(time.perf_counter() - t_start - arrivals[i])
                 done_n += 1
+            t_result += time.perf_counter() - tc
         else:
             time.sleep(0.001)
     t_total = time.perf_counter() - t_start
@@ -541,6 +548,8 @@ def run_serve(args):
             "ligands_per_hour": 3600.0 * nreq / t_total, "latency_p50_s": float(np.percentile(lat, 50)),
             "latency_p99_s": float(np.percentile(lat, 99)), "memory_budget_gb": args.budget_gb,
             "gens_per_tick": args.gens_per_tick, "tick_ms": args.tick_ms, "ticks": int(en.stats().ticks),
+            "host_seconds": {"submit": t_submit, "tick": t_tick, "results": t_result, "total": t_total,
+                             "engine_kernels": en.stats().kernel_s},
             "worker_utilisation": (en.stats().worker_busy_s / en.stats().worker_span_s
                                    if en.stats().worker_span_s > 0 else None)}
 
@@ -574,6 +583,8 @@ def main():
     ap.add_argument("--nreq", type=int, default=200, help="requests (serve mode)")
     ap.add_argument("--budget-gb", type=int, default=8, help="engine device-memory budget (serve mode)")
     ap.add_argument("--gens-per-tick", type=int, default=0, help="generations per engine tick (serve mode; 0: no limit)")
+    ap.add_argument("--rate", type=float, default=0.0,
+                    help="request arrival rate per second (serve mode; 0: 80%% of the measured capacity)")
     ap.add_argument("--tick-ms", type=float, default=50.0, help="wall-clock length of an engine tick (serve mode; 0: none)")
     args = ap.parse_args()
     if args.mode == "ls-kernel":

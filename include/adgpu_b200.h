@@ -371,6 +371,7 @@ typedef struct {
 	 * tick; busy / span is the engine kernel's worker utilisation. */
 	double   worker_busy_s, worker_span_s;
 	uint64_t tasks;
+	double   kernel_s;                /* device time of the engine launches (CUDA events) */
 } adgpu_engine_stats;
 
 adgpu_status adgpu_engine_create(const adgpu_engine_config* cfg, adgpu_engine** out);
