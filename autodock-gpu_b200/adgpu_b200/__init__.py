@@ -5,6 +5,6 @@ and ligand preparation), device (reference kernel API plumbing), dock (plain
 per-ligand docking), engine (batch / serving engine), synth (seeded synthetic
 inputs).  device and dock need torch; the rest do not.
 """
-from . import abi, lib, frontend, engine  # noqa: F401
+from . import abi, lib, frontend, engine, result  # noqa: F401
 
 __all__ = ["abi", "lib", "frontend", "engine"]

@@ -23,6 +23,12 @@ SOURCES = ["adgpu_api.cu", "adgpu_tables.cu", "adgpu_engine.cu", "adgpu_compat.c
 # rounded intrinsics.
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-ftz=true",
               "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-warn-spills"]
+# Result processing restates the reference's host arithmetic operation by
+# operation, so it keeps IEEE denormals and rounds every product and sum
+# separately (no fused multiply-add), as the host code does.
+IEEE_SOURCES = ["adgpu_result.cu"]
+NVCC_FLAGS_IEEE = [f for f in NVCC_FLAGS if f not in ("-ftz=true", "-shared")] + ["-ftz=false", "-fmad=false"]
+OBJ_DIR = os.path.join(HERE, "_build")
 
 
 def nvcc() -> str:
@@ -34,6 +40,15 @@ def nvcc() -> str:
 
 def sources():
     return [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+
+
+def _run(cmd, verbose):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose or r.returncode != 0:
+        sys.stdout.write(r.stdout)
+        sys.stderr.write(r.stderr)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed building libadgpu_b200.so")
 
 
 def needs_rebuild() -> bool:
@@ -49,13 +64,13 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_rebuild():
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT] + sources() + ["-lcudart"]
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if verbose or r.returncode != 0:
-        sys.stdout.write(r.stdout)
-        sys.stderr.write(r.stderr)
-    if r.returncode != 0:
-        raise RuntimeError("nvcc failed building libadgpu_b200.so")
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    objs = []
+    for src in IEEE_SOURCES:
+        obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+        _run([nvcc()] + NVCC_FLAGS_IEEE + ["-c", "-o", obj, os.path.join(CSRC, src)], verbose)
+        objs.append(obj)
+    _run([nvcc()] + NVCC_FLAGS + ["-o", OUT] + sources() + objs + ["-lcudart"], verbose)
     return OUT
 
 

@@ -409,7 +409,6 @@ adgpu_status prepare_ligand(const Grid& grid, const std::string& ligand_text, co
 		rigid_cur = rigid_top;
 		if (f == 0) { true_lig_atoms = (int)atoms.size(); true_lig_rotbonds = (int)branches.size(); }
 	}
-	(void)true_lig_rotbonds;
 	const int N = (int)atoms.size(), NR = (int)branches.size();
 	if (N == 0) return fail(ADGPU_ERR_ARG, "no atoms");
 	if ((int)rotbonds.size() != NR) return fail(ADGPU_ERR_ARG, "BRANCH/ENDBRANCH records unbalanced");
@@ -511,10 +510,18 @@ adgpu_status prepare_ligand(const Grid& grid, const std::string& ligand_text, co
 	const double coeff_vdw = 0.1662, coeff_hb = 0.1209;
 	adgpu_kc_intra& kin = out.intra;
 	memset(&kin, 0, sizeof(kin));
+	PostLigand& pl = out.post;
+	pl.ntypes = NT;
+	pl.reqm_AB.assign(NT * NT, 0.0); pl.vw_A.assign(NT * NT, 0.0); pl.vw_B.assign(NT * NT, 0.0);
+	pl.vw_C.assign(NT * NT, 0.0); pl.vw_D.assign(NT * NT, 0.0); pl.is_hb.assign(NT * NT, 0);
+	pl.vw_index.resize(NT); pl.solpar.resize(NT); pl.volume.resize(NT);
 	for (int t1 = 0; t1 < NT; t1++) {
 		kin.atom_types_reqm_const[t1] = (unsigned)vw[t1];
 		kin.dspars_S_const[t1] = (float)kTypes[vw[t1]].solpar;
 		kin.dspars_V_const[t1] = (float)kTypes[vw[t1]].vol;
+		pl.vw_index[t1] = vw[t1];
+		pl.solpar[t1] = kTypes[vw[t1]].solpar;
+		pl.volume[t1] = kTypes[vw[t1]].vol;
 		for (int t2 = 0; t2 < NT; t2++) {
 			const TypeParams &p1 = kTypes[vw[t1]], &p2 = kTypes[vw[t2]];
 			int idx = t1 * NT + t2;
@@ -526,6 +533,7 @@ adgpu_status prepare_ligand(const Grid& grid, const std::string& ligand_text, co
 				kin.reqm_AB_const[idx] = (float)reqm12;
 				A = 5 * eps12 * pow(reqm12, 12);
 				B = 6 * eps12 * pow(reqm12, 10);
+				pl.reqm_AB[idx] = reqm12; pl.vw_C[idx] = A; pl.vw_D[idx] = B; pl.is_hb[idx] = 1;
 			} else {
 				double eps12 = coeff_vdw * sqrt(p1.eps * p2.eps);
 				double reqm12 = 0.5 * (p1.reqm + p2.reqm);
@@ -533,12 +541,27 @@ adgpu_status prepare_ligand(const Grid& grid, const std::string& ligand_text, co
 				kin.reqm_AB_const[idx] = (float)reqm12;
 				bool cgcg = vw[t1] == kCG && vw[t2] == kCG && types[t1].substr(2) == types[t2].substr(2);
 				if (!cgcg) { A = eps12 * pow(reqm12, 12); B = 2 * eps12 * pow(reqm12, 6); }
+				pl.reqm_AB[idx] = reqm12; pl.vw_A[idx] = A; pl.vw_B[idx] = B;
 			}
 			kin.VWpars_AC_const[idx] = (float)A;
 			kin.VWpars_BD_const[idx] = (float)B;
 		}
 	}
 	(void)kG0;
+
+	pl.natoms = N; pl.true_lig_atoms = true_lig_atoms; pl.nrot = NR; pl.true_lig_rotbonds = true_lig_rotbonds;
+	pl.spacing = grid.spacing;
+	for (int k = 0; k < 3; k++) pl.origin[k] = grid.origin[k];
+	pl.input_xyz.resize(3 * N); pl.charge.resize(N); pl.type.resize(N); pl.map.resize(N);
+	pl.ignore_inter.resize(N); pl.rot_mask.assign(N, 0);
+	for (int i = 0; i < N; i++) {
+		for (int k = 0; k < 3; k++) pl.input_xyz[3 * i + k] = atoms[i].xyz[k];
+		pl.charge[i] = atoms[i].q;
+		pl.type[i] = atoms[i].type;
+		pl.map[i] = map_of_type[atoms[i].type];
+		pl.ignore_inter[i] = atoms[i].ignore_inter ? 1 : 0;
+		for (int r = 0; r < NR; r++) if (atom_rot[i][r]) pl.rot_mask[i] |= 1ull << r;
+	}
 
 	// reference orientation: ligand centred on the origin, flex residues in grid
 	// coordinates, all scaled to grid units (gen_initpop_and_reflig tail)
@@ -572,6 +595,9 @@ adgpu_status prepare_ligand(const Grid& grid, const std::string& ligand_text, co
 	adgpu_kc_conform& cf = out.conform;
 	memset(&cf, 0, sizeof(cf));
 	for (int i = 0; i < N; i++) for (int k = 0; k < 3; k++) cf.ref_coords_const[3 * i + k] = (float)atoms[i].xyz[k];
+	pl.ref_xyz.resize(3 * N);
+	for (int i = 0; i < N; i++) for (int k = 0; k < 3; k++) pl.ref_xyz[3 * i + k] = atoms[i].xyz[k];
+	pl.rot_move.assign(3 * NR, 0.0); pl.rot_unit.assign(3 * NR, 0.0);
 	for (int r = 0; r < NR; r++) {
 		const double* A = atoms[rotbonds[r][0]].xyz;
 		const double* B = atoms[rotbonds[r][1]].xyz;
@@ -589,6 +615,8 @@ adgpu_status prepare_ligand(const Grid& grid, const std::string& ligand_text, co
 			double proj = tt * (B[k] - A[k]) + A[k];
 			cf.rotbonds_moving_vectors_const[3 * r + k] = (float)(proj - 0.0);
 			cf.rotbonds_unit_vectors_const[3 * r + k] = (float)u[k];
+			pl.rot_move[3 * r + k] = proj - 0.0;
+			pl.rot_unit[3 * r + k] = u[k];
 		}
 	}
 	adgpu_kc_grads& gr = out.grads;

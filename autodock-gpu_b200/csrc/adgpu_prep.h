@@ -19,6 +19,29 @@ struct Grid {
 	std::vector<float> values;
 };
 
+// What result processing needs beyond the kernel tables, in the precision the
+// reference's host scorer and pose builder use (double coordinates and pair
+// parameters; host/src/processligand.cpp:1592-1690, 1796-2331): the
+// reference orientation, the coordinates as read, the torsion tree and the
+// per-type-pair van der Waals parameters.
+struct PostLigand {
+	int natoms = 0, true_lig_atoms = 0, nrot = 0, ntypes = 0, true_lig_rotbonds = 0;
+	double origin[3] = {0, 0, 0};         // grid origin, Angstrom
+	double spacing = 0.0;
+	std::vector<double> ref_xyz;          // N*3, grid units, reference orientation
+	std::vector<double> input_xyz;        // N*3, Angstrom, as read from the PDBQT
+	std::vector<double> charge;           // N
+	std::vector<int> type;                // N, ligand type index
+	std::vector<int> map;                 // N, grid map of the type (-1: none)
+	std::vector<uint8_t> ignore_inter;    // N
+	std::vector<uint64_t> rot_mask;       // N, bit r: the atom turns with torsion r
+	std::vector<double> rot_move, rot_unit;          // NR*3, grid units
+	std::vector<double> reqm_AB, vw_A, vw_B, vw_C, vw_D;  // NT*NT
+	std::vector<uint8_t> is_hb;           // NT*NT
+	std::vector<int> vw_index;            // NT: base type index (atom_types_reqm)
+	std::vector<double> solpar, volume;   // NT
+};
+
 // A ligand (plus optional flexible residues) prepared for docking: the tables
 // prepare_const_fields_for_gpu would produce, the initial population and the
 // per-thread LCG seeds of a reference run with the same --seed.
@@ -34,6 +57,7 @@ struct Prepared {
 	int num_rotcyc = 0;
 	std::vector<float> initpop;        // runs * pop_size * 64
 	std::vector<uint32_t> prng;        // runs * pop_size * 64
+	PostLigand post;
 };
 
 }  // namespace adgpu

@@ -331,6 +331,73 @@ adgpu_status adgpu_ligand_population(const adgpu_ligand* lig, float* initpop, si
                                      uint32_t* prng, size_t n_states);
 
 /* ---------------------------------------------------------------------------
+ * Result processing: the output side of the path, on the device.  Replaces
+ * the computations of process_result (host/src/processresult.cpp:1312-1363):
+ * arrange_result (:31-59) orders each run's final population by energy;
+ * make_resfiles (:336-531) rebuilds poses from genotypes (change_conform_f,
+ * host/src/processligand.cpp:1592-1664), re-scores them with the host
+ * scorer (calc_interE_f :1796-2055, calc_intraE_f :2058-2331, with the
+ * IntraTables lookup tables, host/inc/processligand.h:324-364) and takes the
+ * RMSD from the input ligand (calc_rmsd :1441-1489); generate_output
+ * (:655-804) orders the runs by that energy and clusters them by RMSD.  The
+ * .dlg/.xml/.pdbqt writing stays with the caller.  Arithmetic follows the
+ * reference host code operation by operation (IEEE single and double, no
+ * contraction), so the results agree with it to the last bit except where
+ * the device's double sin/cos round differently from the host's.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+	float  rmsd_tolerance;       /* --rmstol, Angstrom (2.0) */
+	int    handle_symmetry;      /* --hsym (1) */
+	int    calc_clustering;      /* --clustering (1) */
+	int    nr_cluster_poses;     /* poses output per cluster (>= 0; 0: all) */
+	int    free_roaming_ligand;  /* 1 for a ligand (cluster energies without intraE), 0 for flexres only */
+	int    rescore_entities;     /* 1: every entity (the final-population report), 0: each run's best only */
+	double coeff_tors;           /* AD4 torsional free-energy coefficient (0.2983, unbound model 0) */
+} adgpu_result_params;
+
+typedef struct {                 /* one run: its best entity after ordering (Ligandresult) */
+	float  inter_e;              /* ligand-receptor (map) energy */
+	float  interflex_e;          /* ligand-flexres energy */
+	float  inter_e_elec;         /* electrostatic part of inter_e */
+	float  intra_e;              /* intramolecular energy */
+	float  intraflex_e;          /* flexres-receptor (map) energy */
+	float  rmsd_from_ref;        /* from the input ligand, Angstrom */
+	float  rmsd_from_cluster_center;
+	float  energy;               /* the population energy (scorer) of the run's best entity */
+	int    run_number;           /* 1-based */
+	int    cluster_id;           /* 1-based; 0 without clustering */
+	int    cluster_subrank;      /* 1-based rank inside the cluster */
+	int    output;               /* pose is output under nr_cluster_poses */
+	int    energy_rank;          /* position of the run in the energy order (0-based) */
+} adgpu_run_result;
+
+typedef struct {
+	int    size;
+	int    best_run;             /* run_number of the cluster's lowest-energy member */
+	double best_energy;          /* kcal/mol, with the torsional term */
+	double sum_energy;           /* over members; mean = sum_energy / size */
+} adgpu_cluster;
+
+adgpu_status adgpu_result_params_default(adgpu_result_params* params);
+
+/* populations (num_runs*pop_size*64 floats) and energies (num_runs*pop_size)
+ * are DEVICE buffers holding the final populations; on return each run's
+ * entities are ordered by energy in place, as arrange_result leaves them.
+ * grid_reference_layout is the DEVICE grid of the kernel API
+ * (adgpu_gpudata.pMem_fgrids).  Host outputs: runs[num_runs]; clusters
+ * (num_runs entries available) with *num_clusters; best_xyz (may be NULL):
+ * num_runs*N*3 doubles, each run's best pose in Angstrom; peratom (may be
+ * NULL): num_runs*N*2 floats (vdW + desolvation, elec) of each best pose, as
+ * make_resfiles reports them per atom; entities (may be
+ * NULL; needs rescore_entities): num_runs*pop_size*3 floats (intra, inter
+ * and RMSD of every entity, as the final-population report prints them). */
+adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_reference_layout,
+                                  float* populations, float* energies, uint32_t num_runs,
+                                  const adgpu_result_params* params, adgpu_run_result* runs,
+                                  adgpu_cluster* clusters, int* num_clusters,
+                                  double* best_xyz, float* peratom, float* entities);
+
+/* ---------------------------------------------------------------------------
  * Layer 2: batch / serving engine (no counterpart in the reference, which
  * docks one ligand at a time through the layer-1 API).
  *

@@ -12,6 +12,7 @@
  *   GpuDockparameters fill                    host/src/performdocking.cpp.Cuda:413-463
  */
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 #include <cstdint>
@@ -21,6 +22,7 @@
 #include "getparameters.h"
 #include "setup.hpp"
 #include "calcenergy.h"
+#include "processresult.h"
 
 /* GpuDockparameters, cuda/GpuData.h:74-110 (kept byte-identical). */
 typedef struct {
@@ -59,6 +61,12 @@ struct RefJob {
 	std::vector<int32_t> bonds;        // [N*N] bond matrix of the prepared ligand
 	std::vector<int32_t> rigid;        // [N] rigid structure ids
 	std::vector<int32_t> contrib;      // [N*N] intramolecular contributor matrix
+	// kept for result processing (process_result's inputs)
+	std::unique_ptr<Liganddata> lig_ref;   // sim_state.myligand_reference
+	std::unique_ptr<Liganddata> lig_init;  // myligand_init (coordinates as read)
+	std::unique_ptr<Liganddata> xray;
+	Dockpars mypars;
+	Gridinfo gridinfo;
 };
 
 /* GpuData layout of cuda/GpuData.h:112-136, with plain pointer members. */
@@ -183,7 +191,11 @@ void* adgpu_ref_job_create(int argc, char** argv)
 			}
 		}
 	}
-	delete lig; delete lig_init; delete xray;
+	job->lig_ref.reset(lig);
+	job->lig_init.reset(lig_init);
+	job->xray.reset(xray);
+	job->mypars = mypars;
+	job->gridinfo = *mygrid;
 	return job;
 }
 
@@ -268,5 +280,105 @@ int adgpu_ref_job_bind(void* h, const void* dockpars_override, uint32_t* prng_st
 }
 
 size_t adgpu_ref_sizeof_refgpudata(void) { return sizeof(RefGpuData); }
+
+/* One run's Ligandresult fields (host/inc/processresult.h:40-58). */
+typedef struct {
+	float inter_e, interflex_e, inter_e_elec, intra_e, intraflex_e, rmsd_from_ref, rmsd_from_cluster_center;
+	int cluster_id, cluster_subrank, output, run_number;
+} adgpu_ref_run_result;
+
+static Dockpars result_pars(const RefJob* j, int num_runs, float rmsd_tol, int symmetry, int clustering, int ncp)
+{
+	Dockpars mp = j->mypars;
+	mp.num_of_runs = num_runs;
+	mp.gen_finalpop = false;
+	mp.gen_best = false;
+	mp.gen_pdbs = 0;
+	mp.output_dlg = false;
+	mp.output_xml = false;
+	mp.contact_analysis = false;
+	mp.xml2dlg = false;
+	mp.rmsd_tolerance = rmsd_tol;
+	mp.handle_symmetry = symmetry != 0;
+	mp.calc_clustering = clustering != 0;
+	mp.nr_cluster_poses = ncp;
+	if (!mp.resname) mp.resname = (char*)"oracle";
+	return mp;
+}
+
+/* process_result (host/src/processresult.cpp:1312-1363) with every file
+ * output switched off: arrange_result + make_resfiles per run, then
+ * generate_output's ordering and clustering.  pops/energies are sorted in
+ * place as the reference sorts them.  xyz: num_runs*N*3 best-pose
+ * coordinates; peratom: num_runs*N*2 (vdW, elec). */
+int adgpu_ref_process_result(void* h, float* pops, float* energies, int num_runs, float rmsd_tol, int symmetry,
+                             int clustering, int ncp, adgpu_ref_run_result* out, double* xyz, float* peratom)
+{
+	RefJob* j = (RefJob*)h;
+	Dockpars mp = result_pars(j, num_runs, rmsd_tol, symmetry, clustering, ncp);
+	const int P = (int)mp.pop_size, N = j->lig_ref->num_of_atoms;
+	IntraTables tables(j->lig_ref.get(), mp.coeffs.scaled_AD4_coeff_elec, mp.coeffs.AD4_coeff_desolv, mp.qasp,
+	                   mp.nr_mod_atype_pairs, mp.mod_atype_pairs);
+	std::vector<Ligandresult> res(num_runs);
+	float best_energy_of_all = 1000000000000.0;
+	int argc = 1;
+	char name[] = "oracle";
+	char* argv[] = {name, nullptr};
+	for (int r = 0; r < num_runs; r++) {
+		float* pr = pops + (size_t)r * P * GENOTYPE_LENGTH_IN_GLOBMEM;
+		float* er = energies + (size_t)r * P;
+		arrange_result(pr, er, P);
+		make_resfiles(pr, er, &tables, j->lig_ref.get(), j->lig_init.get(), j->xray.get(), &mp, 0, 0, &j->gridinfo,
+		              &argc, argv, 0, r, best_energy_of_all, &res[r]);
+	}
+	generate_output(res.data(), num_runs, &tables, j->lig_init.get(), j->xray.get(), &mp, &j->gridinfo, &argc, argv,
+	                0.0, 0, 0, 0.0, 0.0);
+	for (int r = 0; r < num_runs; r++) {
+		const Ligandresult& L = res[r];
+		adgpu_ref_run_result& o = out[r];
+		o.inter_e = L.interE; o.interflex_e = L.interflexE; o.inter_e_elec = L.interE_elec; o.intra_e = L.intraE;
+		o.intraflex_e = L.intraflexE; o.rmsd_from_ref = L.rmsd_from_ref; o.rmsd_from_cluster_center = L.rmsd_from_cluscent;
+		o.cluster_id = L.clus_id; o.cluster_subrank = L.clus_subrank; o.output = L.output ? 1 : 0;
+		o.run_number = L.run_number;
+		for (int a = 0; a < N; a++) {
+			if (xyz) for (int k = 0; k < 3; k++) xyz[((size_t)r * N + a) * 3 + k] = L.atom_idxyzq[a][k + 1];
+			if (peratom) {
+				peratom[((size_t)r * N + a) * 2] = L.peratom_vdw[a];
+				peratom[((size_t)r * N + a) * 2 + 1] = L.peratom_elec[a];
+			}
+		}
+	}
+	return 0;
+}
+
+/* make_resfiles' per-entity body (host/src/processresult.cpp:421-475) for n
+ * genotypes, as the final-population report computes it: out[3*i] =
+ * intraE + intraflexE, out[3*i+1] = interE + interflexE, out[3*i+2] = RMSD
+ * from the input ligand. */
+int adgpu_ref_rescore(void* h, const float* genotypes, int n, int symmetry, float* out)
+{
+	RefJob* j = (RefJob*)h;
+	Dockpars mp = result_pars(j, 1, 2.0f, symmetry, 1, 0);
+	IntraTables tables(j->lig_ref.get(), mp.coeffs.scaled_AD4_coeff_elec, mp.coeffs.AD4_coeff_desolv, mp.qasp,
+	                   mp.nr_mod_atype_pairs, mp.mod_atype_pairs);
+	Liganddata* ref = j->lig_ref.get();
+	const Liganddata* inp = j->lig_init.get();
+	std::unique_ptr<Liganddata> work(new Liganddata(*ref));
+	for (int i = 0; i < n; i++) {
+		memcpy(work->atom_idxyzq, ref->atom_idxyzq, sizeof(ref->atom_idxyzq));
+		change_conform_f(work.get(), &j->gridinfo, genotypes + (size_t)i * GENOTYPE_LENGTH_IN_GLOBMEM, 0);
+		float intraflexE = 0, interflexE = 0;
+		float interE = calc_interE_f(&j->gridinfo, work.get(), 0.0005, 0, intraflexE);
+		scale_ligand(work.get(), j->gridinfo.spacing);
+		float intraE = calc_intraE_f(work.get(), 8, mp.smooth, 0, mp.elec_min_distance, &tables, 0, interflexE);
+		move_ligand(work.get(), j->gridinfo.origo_real_xyz, j->gridinfo.origo_real_xyz);
+		double rmsd = calc_rmsd(inp->atom_idxyzq, work->atom_idxyzq,
+		                        (!inp->true_ligand_atoms) ? inp->num_of_atoms : inp->true_ligand_atoms, mp.handle_symmetry);
+		out[3 * i] = intraE + intraflexE;
+		out[3 * i + 1] = interE + interflexE;
+		out[3 * i + 2] = (float)rmsd;
+	}
+	return 0;
+}
 
 }  // extern "C"

@@ -62,6 +62,8 @@ def lib():
         L.adgpu_ref_autostop_check.restype = C.c_int
         L.adgpu_ref_autostop_check.argtypes = [vp, C.c_int, vp, C.c_ulong]
         L.adgpu_ref_autostop_free.argtypes = [vp]
+        L.adgpu_ref_process_result.argtypes = [vp, vp, vp, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int, vp, vp, vp]
+        L.adgpu_ref_rescore.argtypes = [vp, vp, C.c_int, C.c_int, vp]
         _lib = L
     return _lib
 
@@ -81,6 +83,14 @@ class RefAutoStop:
         if getattr(self, "h", None):
             lib().adgpu_ref_autostop_free(self.h)
             self.h = None
+
+
+class RefRunResult(C.Structure):
+    """One run's Ligandresult fields (host/inc/processresult.h:40-58)."""
+    _fields_ = [("inter_e", C.c_float), ("interflex_e", C.c_float), ("inter_e_elec", C.c_float),
+                ("intra_e", C.c_float), ("intraflex_e", C.c_float), ("rmsd_from_ref", C.c_float),
+                ("rmsd_from_cluster_center", C.c_float), ("cluster_id", C.c_int), ("cluster_subrank", C.c_int),
+                ("output", C.c_int), ("run_number", C.c_int)]
 
 
 def _ptr(a):
@@ -126,6 +136,30 @@ class RefJob:
             self._dp = C.create_string_buffer(bytes(dockpars), len(dockpars))
             dp = C.cast(self._dp, C.c_void_p)
         lib().adgpu_ref_job_bind(self.h, dp, _ptr(prng), _ptr(evals_new), _ptr(evals_runs))
+
+    # --- result processing (host/src/processresult.cpp), files switched off ---
+    def process_result(self, pops: np.ndarray, energies: np.ndarray, rmsd_tol: float = 2.0, symmetry: bool = True,
+                       clustering: bool = True, nr_cluster_poses: int = 0):
+        """Runs arrange_result + make_resfiles per run and generate_output's
+        clustering; returns (sorted pops, sorted energies, runs, xyz, peratom)."""
+        P = self.info.pop_size
+        p = np.ascontiguousarray(pops, np.float32).reshape(-1, GENOTYPE_STRIDE).copy()
+        e = np.ascontiguousarray(energies, np.float32).reshape(-1).copy()
+        R = e.size // P
+        N = self.info.num_of_atoms
+        runs = (RefRunResult * R)()
+        xyz = np.zeros((R, N, 3), np.float64)
+        per = np.zeros((R, N, 2), np.float32)
+        lib().adgpu_ref_process_result(self.h, _ptr(p), _ptr(e), R, rmsd_tol, int(symmetry), int(clustering),
+                                       nr_cluster_poses, C.cast(runs, C.c_void_p), _ptr(xyz), _ptr(per))
+        return p, e, runs, xyz, per
+
+    def rescore(self, genotypes: np.ndarray, symmetry: bool = True) -> np.ndarray:
+        """make_resfiles' per-entity values: [intra, inter, RMSD] per genotype."""
+        g = np.ascontiguousarray(genotypes, np.float32).reshape(-1, GENOTYPE_STRIDE)
+        out = np.zeros((g.shape[0], 3), np.float32)
+        lib().adgpu_ref_rescore(self.h, _ptr(g), g.shape[0], int(symmetry), _ptr(out))
+        return out
 
     # --- emulated reference kernels (host arrays stand in for device memory) ---
     def score(self, genotypes: np.ndarray, gradients: bool, threads: int = NUM_THREADS):
