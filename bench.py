@@ -554,6 +554,83 @@ def run_serve(args):
                                    if en.stats().worker_span_s > 0 else None)}
 
 
+def run_result(args):
+    """--mode result: result processing of one docked ligand of the plain
+    workload (60^3 maps, 40 heavy atoms / 10 torsions, nrun 100, pop 150) on
+    the device (adgpu_process_result: population ordering, re-scoring, RMSD,
+    clustering; host outputs included) against the reference's own
+    process_result on one host core (oracle/_ref, files switched off), on the
+    same final population."""
+    import tempfile
+    import torch
+    from adgpu_b200 import device, dock, frontend, result, synth
+    from oracle import refpy
+    w = WORKLOAD
+    d = tempfile.mkdtemp(prefix="adgpu_result_")
+    spec = synth.grid_spec(w["npts"], w["types"], seed=12345 + w["config_id"])
+    fld = synth.write_maps(spec, synth.make_maps(spec), d)
+    lig_path = os.path.join(d, "ligand.pdbqt")
+    synth.write_ligand(synth.ligand_for(w["config_id"], 0, w["n_heavy"], w["n_tors"]), lig_path)
+    seeds = ",".join(str(s) for s in w["seed"])
+    ref = refpy.RefJob(["--ffile", fld, "--lfile", lig_path, "--nrun", str(w["nrun"]), "--seed", seeds,
+                        "--heuristics", "0", "--autostop", "0", "--psize", str(w["pop"])])
+    grid = frontend.Grid.read(fld)
+    lig = frontend.Ligand(grid, open(lig_path).read(), None, run=frontend.default_dockpars(grid.spacing, w["pop"]),
+                          seed=w["seed"], num_runs=w["nrun"])
+    job = device.DeviceJob(lig.tables, lig.dockpars, grid.reference_layout(), w["nrun"], lig.prng)
+    job.activate()
+    dr = dock.dock(job, lig.initpop, args.lsmet, nev=args.nev)
+    pops0, en0 = dr.conformations.clone(), dr.energies.clone()
+    R = w["nrun"]
+
+    def gpu_time(rescore_all):
+        params = result.default_params(rescore_entities=int(rescore_all))
+        ts, out = [], None
+        for i in range(args.warmup + args.steps):
+            c, e = pops0.clone(), en0.clone()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = result.process_result(lig, job.grid, c, e, R, params)
+            t1 = time.perf_counter()
+            if i >= args.warmup:
+                ts.append(t1 - t0)
+        return statistics.median(ts), out, c, e
+
+    t_best, out, c_sorted, e_sorted = gpu_time(False)
+    t_all, out_all, _, _ = gpu_time(True)
+    hp, he = pops0.cpu().numpy(), en0.cpu().numpy()
+    tr, reps = [], 0
+    t_start = time.perf_counter()
+    while reps < 3 or time.perf_counter() - t_start < 10.0:
+        t0 = time.perf_counter()
+        rp, re_, rruns, rxyz, rper = ref.process_result(hp, he)
+        tr.append(time.perf_counter() - t0)
+        reps += 1
+    t_ref = statistics.median(tr)
+    fields = ("inter_e", "interflex_e", "inter_e_elec", "intra_e", "intraflex_e", "rmsd_from_ref")
+    got = np.array([[getattr(r, f) for f in fields] for r in out.runs], np.float64)
+    want = np.array([[getattr(r, f) for f in fields] for r in rruns], np.float64)
+    same_clusters = all((a.cluster_id, a.cluster_subrank, a.output) == (b.cluster_id, b.cluster_subrank, b.output)
+                        for a, b in zip(out.runs, rruns))
+    exact = float(np.mean(np.concatenate([(got == want).ravel(), (out.best_xyz == rxyz).ravel(),
+                                          (out.peratom == rper).ravel()])))
+    return {"mode": "result", "metric": "ligands/s (result processing)", "workload":
+            f"one docked ligand ({w['n_heavy']} heavy atoms / {w['n_tors']} torsions, {lig.dockpars.num_of_atoms} "
+            f"atoms, {lig.dockpars.num_of_intraE_contributors} pairs), nrun {R}, pop {w['pop']}, {args.lsmet} "
+            f"docking at nev {args.nev}",
+            "gpu_ms_best_entities": 1e3 * t_best, "gpu_ms_all_entities": 1e3 * t_all,
+            "reference_host_ms": 1e3 * t_ref, "reference_reps": reps, "reference_cores": 1,
+            "speedup_vs_reference": t_ref / t_all,
+            "clusters": len(out.clusters), "parity": {
+                "population_order_identical": bool(np.array_equal(c_sorted.cpu().numpy(), rp) and
+                                                   np.array_equal(e_sorted.cpu().numpy(), re_, equal_nan=True)),
+                "clusters_identical": bool(same_clusters),
+                "max_abs_diff": float(np.abs(got - want).max()), "bit_identical_fraction": exact},
+            "note": "the reference re-scores every entity of every run in make_resfiles; the device path does so "
+                    "with rescore_entities (gpu_ms_all_entities, the like-for-like figure) and otherwise only each "
+                    "run's best entity, the only one the .dlg uses"}
+
+
 def _hbm_peak():
     try:
         return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
@@ -570,7 +647,7 @@ def main():
     ap.add_argument("--lsmet", default="ad", choices=["ad", "sw", "adam", "fire"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain sample in the default mode")
-    ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel", "batch", "serve"])
+    ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel", "batch", "serve", "result"])
     ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel mode)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
     ap.add_argument("--engine-tpp", type=int, default=0,
@@ -590,8 +667,8 @@ def main():
     if args.mode == "ls-kernel":
         run_kernel_only(args)
         return
-    if args.mode in ("batch", "serve"):
-        out = run_batch(args) if args.mode == "batch" else run_serve(args)
+    if args.mode in ("batch", "serve", "result"):
+        out = {"batch": run_batch, "serve": run_serve, "result": run_result}[args.mode](args)
         print(json.dumps(out), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
