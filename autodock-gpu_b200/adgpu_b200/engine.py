@@ -40,6 +40,7 @@ SIGNATURES = {
     "adgpu_engine_result": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp, _vp, _vp]),
     "adgpu_engine_stats_get": (C.c_int, [_vp, _vp]),
     "adgpu_engine_request_info": (C.c_int, [_vp, C.c_uint64, _vp, _vp]),
+    "adgpu_engine_process_result": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 lib.SIGNATURES.update(SIGNATURES)
 _bound = False
@@ -74,6 +75,7 @@ class Engine:
         lib.check(_L().adgpu_engine_create(C.byref(cfg), C.byref(h)), "engine_create")
         self.h = h
         self._keep = []
+        self._pop_size = {}
 
     def close(self):
         if getattr(self, "h", None):
@@ -100,6 +102,7 @@ class Engine:
         if st == 5 and not raise_on_budget:
             return None
         lib.check(st, "engine_submit")
+        self._pop_size[rid.value] = ligand.dockpars.pop_size
         return rid.value
 
     def tick(self) -> int:
@@ -131,6 +134,28 @@ class Engine:
                                            ev.ctypes.data_as(_vp), gn.ctypes.data_as(_vp), C.byref(lat)),
                   "engine_result")
         return Result(be, bg, ev, gn, lat.value)
+
+    def process_result(self, request_id: int, natoms: int, params=None, final_population: bool = False):
+        """Result processing of a finished request on the device (ordering,
+        re-scoring, RMSD, clustering); call before result(), which frees the
+        request.  Returns (result.Processed, final populations, final energies)."""
+        from . import result as _res
+        params = params or _res.default_params()
+        _, runs = self.info(request_id)
+        rr = (_res.RunResult * runs)()
+        cl = (_res.Cluster * runs)()
+        nclus = C.c_int()
+        xyz = np.zeros((runs, natoms, 3), np.float64)
+        per = np.zeros((runs, natoms, 2), np.float32)
+        pop = self._pop_size.get(request_id, 0)
+        ent = np.zeros((runs, pop, 3), np.float32) if params.rescore_entities else None
+        fp = np.zeros((runs * pop, abi.GENOTYPE_STRIDE), np.float32) if final_population else None
+        fe = np.zeros(runs * pop, np.float32) if final_population else None
+        ptr = (lambda a: a.ctypes.data_as(_vp) if a is not None else None)
+        lib.check(_L().adgpu_engine_process_result(self.h, request_id, C.byref(params), C.cast(rr, _vp),
+                                                   C.cast(cl, _vp), C.byref(nclus), ptr(xyz), ptr(per), ptr(ent),
+                                                   ptr(fp), ptr(fe)), "engine_process_result")
+        return _res.Processed(list(rr), list(cl)[:nclus.value], xyz, per, ent), fp, fe
 
     def stats(self) -> EngineStats:
         s = EngineStats()

@@ -29,6 +29,7 @@
 
 #include "adgpu_kernels.cuh"
 #include "adgpu_prep.h"
+#include "adgpu_result.h"
 #include "adgpu_tables.h"
 
 namespace adgpu {
@@ -389,6 +390,19 @@ __global__ void __launch_bounds__(kEngineThreads, ADGPU_ENGINE_MIN_CTAS) engine_
 // --------------------------------------------------------------------------
 // host side
 // --------------------------------------------------------------------------
+// Each run's final population (the buffer its last generation wrote) into
+// one contiguous block, the layout result processing takes.
+__global__ void __launch_bounds__(256) gather_final_kernel(ReqDev d, int P, float* conf_out, float* e_out)
+{
+	const int run = blockIdx.x;
+	const int c = d.cur[run];
+	const size_t base = (size_t)run * P;
+	const float* src = d.conf[c] + base * kGenotypeStride;
+	float* dst = conf_out + base * kGenotypeStride;
+	for (int k = threadIdx.x; k < P * kGenotypeStride; k += blockDim.x) dst[k] = src[k];
+	for (int k = threadIdx.x; k < P; k += blockDim.x) e_out[base + k] = d.e[c][base + k];
+}
+
 struct Receptor {
 	float* cells = nullptr;
 	size_t bytes = 0;
@@ -412,6 +426,10 @@ struct Request {
 	// per run: tasks (kind | index bits of the task word) still queued when a
 	// tick's time ran out; they open the run's part of the next tick
 	std::vector<std::vector<uint32_t>> leftover;
+	// result processing inputs (host copies from the prepared ligand)
+	PostLigand post;
+	std::vector<uint32_t> pairs;
+	adgpu_dockpars dp{};
 };
 
 static double now_s()
@@ -669,6 +687,9 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 	r->receptor = rp->receptor;
 	r->runs = runs;
 	r->leftover.assign(runs, {});
+	r->post = lig->p.post;
+	r->pairs = lig->p.pairs;
+	r->dp = dp;
 	r->bytes = need;
 	r->natoms = dp.num_of_atoms;
 	r->ntors = dp.num_of_genes - 6;
@@ -915,6 +936,40 @@ adgpu_status adgpu_engine_result(adgpu_engine* en, uint64_t request_id, float* b
 	E.used -= r.bytes;
 	E.requests.erase(it);
 	return ADGPU_OK;
+}
+
+adgpu_status adgpu_engine_process_result(adgpu_engine* en, uint64_t request_id, const adgpu_result_params* params,
+                                         adgpu_run_result* runs, adgpu_cluster* clusters, int* num_clusters,
+                                         double* best_xyz, float* peratom, float* entities, float* final_population,
+                                         float* final_energies)
+{
+	if (!en || !params) return fail(ADGPU_ERR_ARG, "null argument");
+	Engine& E = en->e;
+	std::lock_guard<std::mutex> lk(E.mu);
+	auto it = E.requests.find(request_id);
+	if (it == E.requests.end()) return fail(ADGPU_ERR_ARG, "unknown request");
+	Request& r = *it->second;
+	if (!r.done) return fail(ADGPU_ERR_STATE, "request still running");
+	const Receptor& R = *E.receptors[r.receptor];
+	const int P = r.dp.pop_size;
+	const size_t npop = (size_t)r.runs * P;
+	void* scratch = nullptr;
+	cudaError_t e = cudaMallocFromPoolAsync(&scratch, npop * (kGenotypeStride + 1) * 4, E.pool, E.stream);
+	if (e != cudaSuccess) return cuda_fail(e, "result gather");
+	float* conf = static_cast<float*>(scratch);
+	float* en_ = conf + npop * kGenotypeStride;
+	gather_final_kernel<<<r.runs, 256, 0, E.stream>>>(r.dev, P, conf, en_);
+	adgpu_status st = process_result_core(r.post, r.pairs.data(), r.dp, R.cells, 1, conf, en_, (uint32_t)r.runs, params,
+	                                      runs, clusters, num_clusters, best_xyz, peratom, entities, E.stream, E.pool);
+	if (st == ADGPU_OK && final_population)
+		e = cudaMemcpyAsync(final_population, conf, npop * kGenotypeStride * 4, cudaMemcpyDeviceToHost, E.stream);
+	if (st == ADGPU_OK && e == cudaSuccess && final_energies)
+		e = cudaMemcpyAsync(final_energies, en_, npop * 4, cudaMemcpyDeviceToHost, E.stream);
+	cudaFreeAsync(scratch, E.stream);
+	cudaError_t e2 = cudaStreamSynchronize(E.stream);
+	if (st != ADGPU_OK) return st;
+	if (e == cudaSuccess) e = e2;
+	return e == cudaSuccess ? ADGPU_OK : cuda_fail(e, "result download");
 }
 
 adgpu_status adgpu_engine_stats_get(adgpu_engine* en, adgpu_engine_stats* out)

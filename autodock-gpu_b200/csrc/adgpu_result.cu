@@ -16,6 +16,7 @@
 #include <cstring>
 #include <vector>
 #include "adgpu_prep.h"
+#include "adgpu_result.h"
 #include "adgpu_tables.h"
 
 namespace adgpu {
@@ -33,7 +34,8 @@ struct PostDev {
 	int N, NL, NR, NT, Q, P;
 	int gx, gy, gz, nmaps;                 // grid points, type maps
 	int rmsd_atoms, symmetry, rescore_all;
-	const float* grid;                     // reference layout, 4 floats per point per map
+	int cells;                             // grid layout: 0 reference (4 floats per point per map), 1 cell records
+	const float* grid;
 	const double *ref_xyz, *input_xyz, *charge, *rot_move, *rot_unit;
 	const double *reqm, *vA, *vB, *vC, *vD, *solpar, *volume;
 	const unsigned long long* rot_mask;
@@ -230,7 +232,22 @@ rescore_kernel(PostDev D, const float* pop, const float* energies, int ntask, Ru
 					kind = 1;
 				} else {
 					const int xl = (int)floorf(x), yl = (int)floorf(y), zl = (int)floorf(z);
-					const float* c0 = D.grid + ((size_t)(unsigned)(xl + yl * D.gx + zl * D.gx * D.gy) << 2);
+					// the 8 corner values of each map in idx_000 .. idx_111 order: 8 consecutive
+					// floats from the point in the reference layout; the cell's record (e, d,
+					// type maps) in the engine's layout, the same values in the same order
+					const float *cv, *ce, *cd;
+					if (D.cells) {
+						const float* rec = D.grid + (size_t)(xl + yl * (D.gx - 1) + zl * (D.gx - 1) * (D.gy - 1)) *
+						                            (size_t)(D.nmaps + 2) * 8;
+						cv = rec + (size_t)(2 + D.map[a]) * 8;
+						ce = rec;
+						cd = rec + 8;
+					} else {
+						const float* c0 = D.grid + ((size_t)(unsigned)(xl + yl * D.gx + zl * D.gx * D.gy) << 2);
+						cv = c0 + (size_t)D.map[a] * g3_4;
+						ce = c0 + (size_t)D.nmaps * g3_4;
+						cd = ce + g3_4;
+					}
 					const float dx = x - xl, omdx = 1.0f - dx;
 					const float dy = y - yl, omdy = 1.0f - dy;
 					const float dz = z - zl, omdz = 1.0f - dz;
@@ -241,12 +258,11 @@ rescore_kernel(PostDev D, const float* pop, const float* energies, int ntask, Ru
 						return c[0] * w[0] + c[1] * w[1] + c[2] * w[2] + c[3] * w[3] + c[4] * w[4] + c[5] * w[5] +
 						       c[6] * w[6] + c[7] * w[7];
 					};
-					const float v = interp(c0 + (size_t)D.map[a] * g3_4);
+					const float v = interp(cv);
 					val += v;
-					const float* ce = c0 + (size_t)D.nmaps * g3_4;
 					e = q * interp(ce);
 					val += e;
-					const float ed = fabsf(q) * interp(ce + g3_4);
+					const float ed = fabsf(q) * interp(cd);
 					val += ed;
 					// AD4_desolv_peratom_vdW is defined (host/src/processligand.cpp:30, 2041-2043)
 					vd = v + ed;
@@ -543,16 +559,18 @@ adgpu_status adgpu_result_params_default(adgpu_result_params* p)
 	return ADGPU_OK;
 }
 
-adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_reference_layout, float* populations,
-                                  float* energies, uint32_t num_runs, const adgpu_result_params* params,
-                                  adgpu_run_result* runs_out, adgpu_cluster* clusters_out, int* num_clusters,
-                                  double* best_xyz, float* peratom, float* entities)
+}  // extern "C"
+
+namespace adgpu {
+
+adgpu_status process_result_core(const PostLigand& L, const uint32_t* pairs, const adgpu_dockpars& dp,
+                                 const float* grid, int grid_cells, float* populations, float* energies,
+                                 uint32_t num_runs, const adgpu_result_params* params, adgpu_run_result* runs_out,
+                                 adgpu_cluster* clusters_out, int* num_clusters, double* best_xyz, float* peratom,
+                                 float* entities, cudaStream_t st, cudaMemPool_t pool)
 {
-	if (!lig || !grid_reference_layout || !populations || !energies || !params || !runs_out || !clusters_out ||
-	    !num_clusters)
+	if (!grid || !populations || !energies || !params || !runs_out || !clusters_out || !num_clusters)
 		return fail(ADGPU_ERR_ARG, "null argument");
-	const PostLigand& L = lig->p.post;
-	const adgpu_dockpars& dp = lig->p.dockpars;
 	if (num_runs == 0 || num_runs > ADGPU_MAX_RUNS) return fail(ADGPU_ERR_LIMIT, "num_runs must be 1..8192");
 	if (L.natoms <= 0) return fail(ADGPU_ERR_STATE, "ligand carries no result-processing data");
 	if (params->nr_cluster_poses < 0)
@@ -577,7 +595,7 @@ adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_ref
 	             o_mask = put(blob, L.rot_mask.data(), N), o_tab = put(blob, tab.data(), tab.size()),
 	             o_qa = put(blob, qabs.data(), N), o_ty = put(blob, L.type.data(), N), o_map = put(blob, L.map.data(), N),
 	             o_vw = put(blob, L.vw_index.data(), NT), o_ig = put(blob, L.ignore_inter.data(), N),
-	             o_hb = put(blob, L.is_hb.data(), NT * NT), o_pr = put(blob, lig->p.pairs.data(), 2 * (size_t)Q);
+	             o_hb = put(blob, L.is_hb.data(), NT * NT), o_pr = put(blob, pairs, 2 * (size_t)Q);
 	// device scratch
 	const size_t n_pop = (size_t)R * P * 64;
 	size_t off = (blob.size() + 255) / 256 * 256;
@@ -588,16 +606,13 @@ adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_ref
 	             o_cr = take((size_t)R * 8), o_cl = take((size_t)R * sizeof(adgpu_cluster)), o_nc = take(4);
 
 	unsigned char* d = nullptr;
-	cudaStream_t st = nullptr;
-	cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-	if (e != cudaSuccess) return cuda_fail(e, "stream");
 	auto done = [&](cudaError_t err, const char* what) {
 		if (d) cudaFreeAsync(d, st);
 		cudaStreamSynchronize(st);
-		cudaStreamDestroy(st);
 		return err == cudaSuccess ? ADGPU_OK : cuda_fail(err, what);
 	};
-	e = cudaMallocAsync(reinterpret_cast<void**>(&d), off, st);
+	cudaError_t e = pool ? cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d), off, pool, st)
+	                     : cudaMallocAsync(reinterpret_cast<void**>(&d), off, st);
 	if (e != cudaSuccess) { d = nullptr; return done(e, "result scratch"); }
 	e = cudaMemcpyAsync(d, blob.data(), blob.size(), cudaMemcpyHostToDevice, st);
 	if (e != cudaSuccess) return done(e, "result tables");
@@ -609,7 +624,8 @@ adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_ref
 	D.rmsd_atoms = L.true_lig_atoms ? L.true_lig_atoms : N;
 	D.symmetry = params->handle_symmetry ? 1 : 0;
 	D.rescore_all = params->rescore_entities ? 1 : 0;
-	D.grid = grid_reference_layout;
+	D.cells = grid_cells ? 1 : 0;
+	D.grid = grid;
 	D.ref_xyz = (const double*)(d + o_ref); D.input_xyz = (const double*)(d + o_in); D.charge = (const double*)(d + o_q);
 	D.rot_move = (const double*)(d + o_mv); D.rot_unit = (const double*)(d + o_un);
 	D.reqm = (const double*)(d + o_reqm); D.vA = (const double*)(d + o_A); D.vB = (const double*)(d + o_B);
@@ -671,6 +687,27 @@ adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_ref
 		o.energy_rank = s.rank;
 	}
 	return done(cudaSuccess, "");
+}
+
+
+}  // namespace adgpu
+
+extern "C" {
+
+adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_reference_layout, float* populations,
+                                  float* energies, uint32_t num_runs, const adgpu_result_params* params,
+                                  adgpu_run_result* runs_out, adgpu_cluster* clusters_out, int* num_clusters,
+                                  double* best_xyz, float* peratom, float* entities)
+{
+	if (!lig) return fail(ADGPU_ERR_ARG, "null argument");
+	cudaStream_t st = nullptr;
+	cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+	if (e != cudaSuccess) return cuda_fail(e, "stream");
+	adgpu_status rc = process_result_core(lig->p.post, lig->p.pairs.data(), lig->p.dockpars, grid_reference_layout, 0,
+	                                      populations, energies, num_runs, params, runs_out, clusters_out, num_clusters,
+	                                      best_xyz, peratom, entities, st, nullptr);
+	cudaStreamDestroy(st);
+	return rc;
 }
 
 }  // extern "C"

@@ -460,6 +460,15 @@ adgpu_status adgpu_engine_poll(adgpu_engine* engine, uint64_t request_id, int* d
  * submit-to-finish latency.  Frees the request's device state. */
 adgpu_status adgpu_engine_result(adgpu_engine* engine, uint64_t request_id, float* best_energies,
                                  float* best_genotypes, int* evals, uint32_t* generations, double* latency_s);
+/* adgpu_process_result on a finished request's final populations (call it
+ * before adgpu_engine_result, which frees them); the request's ligand and
+ * the receptor's resident maps are used.  final_population (runs*pop*64
+ * floats) and final_energies (runs*pop), host, may be NULL: the populations
+ * ordered as arrange_result leaves them. */
+adgpu_status adgpu_engine_process_result(adgpu_engine* engine, uint64_t request_id, const adgpu_result_params* params,
+                                         adgpu_run_result* runs, adgpu_cluster* clusters, int* num_clusters,
+                                         double* best_xyz, float* peratom, float* entities, float* final_population,
+                                         float* final_energies);
 adgpu_status adgpu_engine_stats_get(adgpu_engine* engine, adgpu_engine_stats* out);
 /* Threads per pose the engine chose for a request, and its run count. */
 adgpu_status adgpu_engine_request_info(adgpu_engine* engine, uint64_t request_id, int* threads_per_pose, int* runs);

@@ -154,3 +154,24 @@ def test_process_result_argument_errors(tmp_path):
         result.process_result(L, grid_dev, dp, de, 2, result.default_params(nr_cluster_poses=-1))
     with pytest.raises(Exception):
         result.process_result(L, grid_dev, dp, de, 0)
+
+
+def test_engine_process_result_matches_reference(tmp_path):
+    """The engine's result processing (resident cell-record maps, final
+    populations gathered from its double buffers) on a docked request, against
+    the reference's process_result on the same final populations."""
+    from adgpu_b200 import engine
+    case = helpers.make_case(str(tmp_path), 40, synth.MAP_TYPES_5, 16, 4, 8, config_id=1)
+    L, _ = product_inputs(tmp_path, case)
+    g = frontend.Grid.read(str(tmp_path / "receptor.maps.fld"))
+    en = engine.Engine(memory_budget_bytes=1 << 30)
+    rec = en.add_receptor(g)
+    rid = en.submit(L, rec, "ad", max_evals=60_000)
+    en.run()
+    out, fp, fe = en.process_result(rid, case.info.num_of_atoms, final_population=True)
+    en.result(rid)
+    assert np.all(np.diff(fe.reshape(case.runs, -1), axis=1) >= 0)      # ordered per run
+    ref_pops, ref_en, ref_runs, ref_xyz, ref_per = case.job.process_result(fp, fe)
+    assert np.array_equal(ref_pops, fp) and np.array_equal(ref_en, fe)   # already in arrange_result's order
+    check_against_reference((ref_pops, ref_en, ref_runs, ref_xyz, ref_per), out, fp, fe, case.runs)
+    en.close()
