@@ -542,6 +542,7 @@ def run_serve(args):
     ligs = [frontend.Ligand(grids[t], texts[i], None, run=frontend.default_dockpars(grids[t].spacing, 150),
                             seed=w["seed"], num_runs=nrun) for i, t in enumerate(targets)]
     budget = args.budget_gb << 30
+    natoms = [lg.dockpars.num_of_atoms for lg in ligs]
     # capacity: a batch of requests run to completion in one launch
     cap_n = min(nreq, 48)
     cap = engine.Engine(memory_budget_bytes=budget)
@@ -583,6 +584,8 @@ def run_serve(args):
             t_tick += tc - tb
             for rid in [r for r in live if en.done(r)]:
                 i = live.pop(rid)
+                if args.process_results:
+                    en.process_result(rid, natoms[i])
                 en.result(rid)
                 lat.append(time.perf_counter() - t_start - arrivals[i])
                 done_n += 1
@@ -597,6 +600,7 @@ def run_serve(args):
             "ligands_per_hour": 3600.0 * nreq / t_total, "latency_p50_s": float(np.percentile(lat, 50)),
             "latency_p99_s": float(np.percentile(lat, 99)), "memory_budget_gb": args.budget_gb,
             "gens_per_tick": args.gens_per_tick, "tick_ms": args.tick_ms, "ticks": int(en.stats().ticks),
+            "results_processed_on_device": bool(args.process_results),
             "host_seconds": {"submit": t_submit, "tick": t_tick, "results": t_result, "total": t_total,
                              "engine_kernels": en.stats().kernel_s},
             "worker_utilisation": (en.stats().worker_busy_s / en.stats().worker_span_s
@@ -709,6 +713,8 @@ def main():
     ap.add_argument("--nreq", type=int, default=200, help="requests (serve mode)")
     ap.add_argument("--budget-gb", type=int, default=8, help="engine device-memory budget (serve mode)")
     ap.add_argument("--gens-per-tick", type=int, default=0, help="generations per engine tick (serve mode; 0: no limit)")
+    ap.add_argument("--process-results", action="store_true",
+                    help="serve mode: each finished request's runs ordered, re-scored and clustered on the device")
     ap.add_argument("--rate", type=float, default=0.0,
                     help="request arrival rate per second (serve mode; 0: 80%% of the measured capacity)")
     ap.add_argument("--tick-ms", type=float, default=50.0, help="wall-clock length of an engine tick (serve mode; 0: none)")
