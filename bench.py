@@ -246,6 +246,20 @@ def _config(args):
             "parallelism": f"replicas x{args.gpus}"}
 
 
+def rank_aggregate(seconds: float, work: float, device, world: int):
+    """Whole-job figures of a replicas run: the slowest rank's timed seconds
+    (max over ranks) and the work of all ranks (sum), through
+    torch.distributed (NCCL on the GPUs; any backend works)."""
+    if world <= 1:
+        return float(seconds), float(work)
+    import torch
+    t = torch.tensor([float(seconds)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    w = torch.tensor([float(work)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
+    return float(t.item()), float(w.item())
+
+
 def run_engine(args, rank, world, local_rank):
     import torch
     from adgpu_b200 import device, dock, lib
@@ -289,14 +303,8 @@ def run_engine(args, rank, world, local_rank):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     t_local = sum(times)
-    t_all = t_local
-    ev_all = evals
-    if world > 1:
-        t = torch.tensor([t_local], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e = torch.tensor([float(evals)], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(e, op=torch.distributed.ReduceOp.SUM)
-        t_all, ev_all = float(t.item()), int(e.item())
+    t_all, ev_all = rank_aggregate(t_local, evals, dev, world)
+    ev_all = int(ev_all)
     value = ev_all / t_all
     best = float(res.energies.min().item())
 
@@ -323,14 +331,8 @@ def run_engine(args, rank, world, local_rank):
         d2h = conf_h.nbytes + en_h.nbytes + r2.evals_per_run.nbytes
         del j2
     job.activate()
-    e2e_local = sum(e2e_times)
-    e2e_value = e2e_evals / e2e_local
-    if world > 1:
-        t = torch.tensor([e2e_local], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e = torch.tensor([float(e2e_evals)], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(e, op=torch.distributed.ReduceOp.SUM)
-        e2e_value = float(e.item()) / float(t.item())
+    e2e_t, e2e_all = rank_aggregate(sum(e2e_times), e2e_evals, dev, world)
+    e2e_value = e2e_all / e2e_t
 
     # --- roofline of the dominant kernel (the local search) -------------------------
     cm = cost_model(lig)
