@@ -175,3 +175,18 @@ def test_engine_process_result_matches_reference(tmp_path):
     assert np.array_equal(ref_pops, fp) and np.array_equal(ref_en, fe)   # already in arrange_result's order
     check_against_reference((ref_pops, ref_en, ref_runs, ref_xyz, ref_per), out, fp, fe, case.runs)
     en.close()
+
+
+def test_process_result_maximum_size(tmp_path):
+    """252 atoms, 57 torsions, 29,104 pairs: the largest ligand the reference
+    accepts, runs clustered around two poses near the input conformation."""
+    case = helpers.make_case(str(tmp_path), 80, synth.MAP_TYPES_5, 226, 57, 6, config_id=3)
+    R, P = case.runs, case.info.pop_size
+    rng = np.random.default_rng(6)
+    base = helpers.in_box_genotypes(case, 2, seed=8, spread=1.0)
+    base[:, 6:case.ngenes] = rng.normal(0.0, 5.0, (2, case.ngenes - 6)).astype(np.float32)
+    pops = np.repeat(base[np.arange(R) % 2], P, axis=0).copy()
+    pops[:, :case.ngenes] += rng.normal(0.0, 0.05, (R * P, case.ngenes)).astype(np.float32)
+    en = rng.normal(-6.0, 2.0, R * P).astype(np.float32)
+    ref, out, dev_pops, dev_en, _, _ = run_both(tmp_path, case, pops, en)
+    check_against_reference(ref, out, dev_pops, dev_en, R)

@@ -82,3 +82,21 @@ def test_large_ligand_parity(tmp_path):
     ng = case.ngenes
     assert np.all(np.abs(gr_gpu[:, :ng] - gr_ref[:, :ng]) <= helpers.gradient_bound(case, gr_ref))
     del dj
+
+
+def test_maximum_size_parity(tmp_path):
+    """At the reference's limits: 252 atoms (226 heavy plus polar H), 57
+    torsions (MAX_NUM_OF_ROTBONDS), 29,104 intramolecular pairs, 80^3 maps;
+    poses near the input conformation so that the terms stay finite."""
+    from adgpu_b200 import device
+    case = helpers.make_case(str(tmp_path / "max"), 80, ["C", "A", "N", "OA", "HD"], 226, 57, 2, config_id=3)
+    assert case.info.num_of_rotbonds == 57 and case.info.num_of_atoms > 240
+    dj = _activate(case)
+    g = helpers.in_box_genotypes(case, 200, seed=3, spread=1.0)
+    g[:, 6:case.ngenes] = np.random.default_rng(4).normal(0.0, 5.0, (200, case.ngenes - 6)).astype(np.float32)
+    e_gpu, gr_gpu = device.score(g, True)
+    e_ref, gr_ref = case.host.score(g, True, nthreads=8)
+    assert np.all(np.abs(e_gpu - e_ref) <= helpers.energy_tolerance(e_ref)), np.abs(e_gpu - e_ref).max()
+    ng = case.ngenes
+    assert np.all(np.abs(gr_gpu[:, :ng] - gr_ref[:, :ng]) <= helpers.gradient_bound(case, gr_ref))
+    del dj
