@@ -191,15 +191,20 @@ adgpu_status launch_lga(const KArgs& a, float* grads, cudaStream_t stream, int c
 	return ADGPU_OK;
 }
 
-// Threads per pose for a launch of n blocks when none is configured.  Local
-// searches: 64.  A local-search launch ends with its longest entities running
-// alone, and two warps per pose halve that tail; on B200, 64 beat 32 and 128
-// for per-ligand dockings of 20 and of 100 runs (80% local-search rate,
-// 10-64 heavy atoms).  Other kernels: 64 when every block still gets a
-// resident pose group of 64 threads (6 CTAs of 128 threads per SM), else 32.
-static int auto_tpp(uint32_t n, bool local_search)
+// Threads per pose for a launch of n blocks when none is configured.
+// Solis-Wets and ADADELTA: 64.  Their searches stop on their own step-size
+// test, so a launch ends with its longest entities running alone, and two
+// warps per pose halve that tail; on B200, 64 beat 32 and 128 for per-ligand
+// dockings of 20 and of 100 runs (80% local-search rate, 10-64 heavy atoms;
+// 100 runs of 40 heavy atoms: ADADELTA 121 vs 116 M evals/s, Solis-Wets 242
+// vs 232).  ADAM and FIRE run a fixed number of iterations, so there is no
+// tail to shorten and throughput decides: 32 (ADAM 163 vs 146, FIRE 138 vs
+// 119 M evals/s at 100 runs) unless the launch leaves pose groups idle.
+// Other kernels: 64 when every block still gets a resident pose group of 64
+// threads (6 CTAs of 128 threads per SM), else 32.
+static int auto_tpp(uint32_t n, int kind)
 {
-	if (local_search) return 64;
+	if (kind == 1 || kind == 2) return 64;
 	if (g_num_sms == 0) {
 		int dev = 0;
 		if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -212,7 +217,7 @@ static int auto_tpp(uint32_t n, bool local_search)
 template <int KIND>
 adgpu_status launch_kind(const KArgs& a, float* grads, cudaStream_t stream, int tpp)
 {
-	if (tpp == 0) tpp = auto_tpp(a.nblocks, KIND >= 1 && KIND <= 4);
+	if (tpp == 0) tpp = auto_tpp(a.nblocks, KIND);
 	switch (tpp) {
 	case 32: return launch_lga<32, KIND>(a, grads, stream, 128);
 	case 64: return launch_lga<64, KIND>(a, grads, stream, 128);
