@@ -308,13 +308,19 @@ template <int TPP, bool GRAD>
 __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, int rank)
 {
 	constexpr uint32_t k12_6 = 12u | (6u << 8), k12_10 = 12u | (10u << 8);
+	// loop invariants read once: when L lives in shared memory (the engine's
+	// per-task arguments) the force atomics below would otherwise force a
+	// reload of every field in every iteration
 	const float hs = L.half_smooth, emd = L.elec_min_distance;
 	const float inv_emd = __fdividef(1.0f, emd);
+	const int npairs = L.npairs;
+	const PairRec* const pairs = L.pairs;
+	const float spacing = L.spacing, inv_spacing = L.inv_spacing, coeff_desolv = L.coeff_desolv;
 	float2 esum = f2s(0.0f);
-	for (int p = rank; p < L.npairs; p += 2 * TPP) {
-		const bool has_b = p + TPP < L.npairs;       // the second pair; else pair a twice, b discarded
-		const float4* pra = reinterpret_cast<const float4*>(L.pairs + p);
-		const float4* prb = reinterpret_cast<const float4*>(L.pairs + (has_b ? p + TPP : p));
+	for (int p = rank; p < npairs; p += 2 * TPP) {
+		const bool has_b = p + TPP < npairs;          // the second pair; else pair a twice, b discarded
+		const float4* pra = reinterpret_cast<const float4*>(pairs + p);
+		const float4* prb = reinterpret_cast<const float4*>(pairs + (has_b ? p + TPP : p));
 		const float4 Aa = __ldg(pra), Ba = __ldg(pra + 1), Ab = __ldg(prb), Bb = __ldg(prb + 1);
 		const uint32_t ija = __float_as_uint(Ba.z), ijb = __float_as_uint(Bb.z);
 		const int a1 = ija & 0xFF, a2 = (ija >> 8) & 0xFF, b1 = ijb & 0xFF, b2 = (ijb >> 8) & 0xFF;
@@ -325,7 +331,7 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 		const float2 d2g = f2fma(sz, sz, f2fma(sy, sy, f2mul(sx, sx)));
 		// coincident atoms (d2g = 0) get r = 0 from a finite reciprocal
 		const float2 inv_dist = f2(rsqrtf(fmaxf(d2g.x, 1e-30f)), rsqrtf(fmaxf(d2g.y, 1e-30f)));
-		const float2 r = f2mul(f2mul(d2g, inv_dist), f2s(L.spacing));
+		const float2 r = f2mul(f2mul(d2g, inv_dist), f2s(spacing));
 		const float2 vbond = f2(Ba.y, Bb.y);          // G for CG-G0 pairs, else 0
 		float2 e = f2mul(vbond, r);
 		float2 pg = vbond;
@@ -367,14 +373,14 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 		// electrostatics and desolvation, cut-off 20.48 A
 		{
 			const float2 in20 = f2(lt1(r.x, 20.48f), lt1(r.y, 20.48f));
-			float2 inv_r = f2mul(inv_dist, f2s(L.inv_spacing));
+			float2 inv_r = f2mul(inv_dist, f2s(inv_spacing));
 			float2 rr = r;
 			if (rr.x < emd) { rr.x = emd; inv_r.x = inv_emd; }
 			if (rr.y < emd) { rr.y = emd; inv_r.y = inv_emd; }
 			const float2 d2 = f2mul(rr, rr);
 			const float2 num = f2fma(f2mul(f2s(-0.1063f), d2), f2fma(f2s(-0.001947f), d2, f2s(1.0f)), f2s(12.96f));
 			const float2 den = f2fma(d2, f2fma(d2, f2fma(f2s(0.000112f), d2, f2s(0.00357f)), f2s(0.4137f)), f2s(12.96f));
-			const float2 cn = f2mul(f2s(L.coeff_desolv), num);
+			const float2 cn = f2mul(f2s(coeff_desolv), num);
 			const float2 desolv = f2mul(f2(Aa.w, Ab.w), f2(__fdividef(cn.x, den.x), __fdividef(cn.y, den.y)));
 			const float2 rs = f2(__fdividef(1.0f, rr.x + 1.26366f), __fdividef(1.0f, rr.y + 1.26366f));
 			const float2 rs2 = f2mul(rs, rs);
