@@ -187,27 +187,35 @@ struct Group {
 		}
 	}
 
-	// Six sums in one pass (torque x,y,z and force x,y,z).
-	__device__ __forceinline__ void sum6(float* v) const
+	// K <= 8 sums in one pass, each added in the same order as sum() adds a
+	// single value.  scratch_free: the caller has just passed a group barrier
+	// after the scratch's last readers, so the leading barrier is skipped.
+	template <int K>
+	__device__ __forceinline__ void sum_n(float* v, bool scratch_free = false) const
 	{
 #pragma unroll
-		for (int k = 0; k < 6; k++) {
+		for (int k = 0; k < K; k++) {
 #pragma unroll
 			for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
 		}
 		if constexpr (TPP != 32) {
 			const int w = rank >> 5;
-			sync();
+			if (!scratch_free) sync();
 			if ((rank & 31) == 0)
-				for (int k = 0; k < 6; k++) red[w * 8 + k] = v[k];
+#pragma unroll
+				for (int k = 0; k < K; k++) red[w * 8 + k] = v[k];
 			sync();
-			for (int k = 0; k < 6; k++) {
+#pragma unroll
+			for (int k = 0; k < K; k++) {
 				float s = 0.0f;
 				for (int i = 0; i < TPP / 32; i++) s += red[i * 8 + k];
 				v[k] = s;
 			}
 		}
 	}
+
+	// Six sums in one pass (torque x,y,z and force x,y,z).
+	__device__ __forceinline__ void sum6(float* v) const { sum_n<6>(v); }
 };
 
 // ---- per-pose shared-memory scratch -------------------------------------------------
@@ -534,12 +542,12 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 
 	// 4. intramolecular pairs (cuda/calcMergeEneGra.cu:418-602)
 	e_acc += pair_terms<TPP, GRAD>(L, S, rank);
-	const float energy = G.sum(e_acc);
-	if (!GRAD) return energy;
-	G.sync();
+	if (!GRAD) return G.sum(e_acc);
+	G.sync();   // every pair's forces are in S.fx/fy/fz
 
-	// 5. torque and total force over the ligand atoms (cuda/calcMergeEneGra.cu:608-661)
-	float red[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+	// 5. torque and total force over the ligand atoms (cuda/calcMergeEneGra.cu:608-661);
+	//    the energy rides along as a seventh sum (one cross-warp exchange, not two)
+	float red[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, e_acc};
 	for (int a = rank; a < L.nlig; a += TPP) {
 		const float4 pa = S.xyz[a];
 		float3 r = make_float3((pa.x - gr.mv.x) * L.spacing, (pa.y - gr.mv.y) * L.spacing, (pa.z - gr.mv.z) * L.spacing);
@@ -548,7 +556,8 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 		float3 t = cross3(r, f);
 		red[0] += t.x; red[1] += t.y; red[2] += t.z;
 	}
-	G.sum6(red);
+	G.template sum_n<7>(red, true);
+	const float energy = red[6];
 	if (rank == 0 && L.nlig > 0) {
 		// translation (:676-689) and orientation (:695-815) genes
 		S.gg[0] = quant(red[3] * L.spacing);
