@@ -31,6 +31,17 @@ class Grid:
         return cls(h)
 
     @classmethod
+    def load(cls, cache_path: str) -> "Grid":
+        """A grid from its binary cache (see save)."""
+        h = C.c_void_p()
+        lib.check(lib.load().adgpu_grid_load(cache_path.encode(), C.byref(h)), f"grid_load {cache_path}")
+        return cls(h)
+
+    def save(self, cache_path: str) -> None:
+        """Writes the parsed maps as a binary cache that load() reads in one pass."""
+        lib.check(lib.load().adgpu_grid_save(self.h, cache_path.encode()), f"grid_save {cache_path}")
+
+    @classmethod
     def from_maps(cls, maps: dict, types: list, spacing: float, origin) -> "Grid":
         """maps: {type: float32 [z, y, x]} for the type maps and 'e', 'd'."""
         order = list(types) + ["e", "d"]
@@ -79,6 +90,32 @@ class Ligand:
             grid.h, ligand_pdbqt.encode() if ligand_pdbqt else None,
             flexres_pdbqt.encode() if flexres_pdbqt else None, C.byref(run), s, num_runs, C.byref(h)),
             "ligand_prepare")
+        self._adopt(h, num_runs)
+
+    @classmethod
+    def prepare_batch(cls, grid: Grid, ligand_pdbqts, flexres_pdbqt: str | None = None, run: abi.Dockpars | None = None,
+                      seeds=None, num_runs: int = 10, nthreads: int = 0) -> list:
+        """Prepares many ligands on nthreads host threads (0: all cores); seeds:
+        one (a, b, c) triple per ligand (default: the same triple for all)."""
+        run = run or default_dockpars(grid.spacing)
+        n = len(ligand_pdbqts)
+        seeds = seeds or [(305419896, 2271560481, 3735928559)] * n
+        texts = (C.c_char_p * n)(*[t.encode() if t else None for t in ligand_pdbqts])
+        flex = (C.c_char_p * n)(*([flexres_pdbqt.encode()] * n)) if flexres_pdbqt else None
+        sd = (C.c_uint32 * (3 * n))(*[int(x) for s in seeds for x in s])
+        out = (C.c_void_p * n)()
+        st = (C.c_int * n)()
+        rc = lib.load().adgpu_ligand_prepare_batch(grid.h, texts, flex, n, C.byref(run), sd, num_runs, nthreads, out, st)
+        ligs = []
+        for i in range(n):
+            if out[i]:
+                lg = cls.__new__(cls)
+                lg._adopt(C.c_void_p(out[i]), num_runs)
+                ligs.append(lg)
+        lib.check(rc, "ligand_prepare_batch")
+        return ligs
+
+    def _adopt(self, h, num_runs: int):
         self.h = h
         self.num_runs = num_runs
         self.dockpars = abi.Dockpars()

@@ -35,6 +35,9 @@ SIGNATURES = {
     "adgpu_grid_read": (_i, [C.c_char_p, _vp]),
     "adgpu_grid_from_values": (_i, [_vp, C.c_double, _vp, _i, _vp, _vp, _vp]),
     "adgpu_grid_free": (None, [_vp]),
+    "adgpu_grid_save": (_i, [_vp, C.c_char_p]),
+    "adgpu_grid_load": (_i, [C.c_char_p, _vp]),
+    "adgpu_ligand_prepare_batch": (_i, [_vp, _vp, _vp, C.c_uint32, _vp, _vp, _i, _i, _vp, _vp]),
     "adgpu_grid_info": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "adgpu_grid_reference_layout": (_i, [_vp, _vp, C.c_size_t]),
     "adgpu_dockpars_default": (_i, [_vp, C.c_double, _i]),

@@ -1,6 +1,11 @@
 // adgpu_frontend.cpp -- C ABI of the front end (include/adgpu_b200.h).
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
+#include <string>
+#include <thread>
+#include <vector>
 #include "adgpu_prep.h"
 
 namespace adgpu {
@@ -43,6 +48,23 @@ adgpu_status adgpu_grid_from_values(const int dims[3], double spacing, const dou
 }
 
 void adgpu_grid_free(adgpu_grid* grid) { delete grid; }
+
+adgpu_status adgpu_grid_save(const adgpu_grid* grid, const char* path)
+{
+	if (!grid || !path) return fail(ADGPU_ERR_ARG, "null argument");
+	return grid_save(grid->g, path);
+}
+
+adgpu_status adgpu_grid_load(const char* path, adgpu_grid** out)
+{
+	if (!path || !out) return fail(ADGPU_ERR_ARG, "null argument");
+	adgpu_grid* g = new (std::nothrow) adgpu_grid;
+	if (!g) return fail(ADGPU_ERR_ARG, "out of host memory");
+	adgpu_status st = grid_load(path, g->g);
+	if (st != ADGPU_OK) { delete g; return st; }
+	*out = g;
+	return ADGPU_OK;
+}
 
 adgpu_status adgpu_grid_info(const adgpu_grid* grid, int dims[3], double* spacing, double origin[3], int* num_map_atypes)
 {
@@ -93,6 +115,41 @@ adgpu_status adgpu_ligand_prepare(const adgpu_grid* grid, const char* ligand_pdb
 }
 
 void adgpu_ligand_free(adgpu_ligand* lig) { delete lig; }
+
+adgpu_status adgpu_ligand_prepare_batch(const adgpu_grid* grid, const char* const* ligand_pdbqt,
+                                        const char* const* flexres_pdbqt, uint32_t count, const adgpu_dockpars* run,
+                                        const uint32_t* seeds, int num_runs, int nthreads, adgpu_ligand** out,
+                                        adgpu_status* status)
+{
+	if (!grid || !ligand_pdbqt || !run || !seeds || !out || !status) return fail(ADGPU_ERR_ARG, "null argument");
+	if (num_runs < 0 || num_runs > ADGPU_MAX_RUNS) return fail(ADGPU_ERR_LIMIT, "num_runs must be 0..8192");
+	if (run->pop_size < 2 || run->pop_size > ADGPU_MAX_POPSIZE) return fail(ADGPU_ERR_LIMIT, "pop_size must be 2..2048");
+	for (uint32_t i = 0; i < count; i++) { out[i] = nullptr; status[i] = ADGPU_ERR_STATE; }
+	unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+	unsigned nt = nthreads > 0 ? (unsigned)nthreads : hw;
+	nt = std::max(1u, std::min<unsigned>(nt, count));
+	std::atomic<uint32_t> next(0);
+	auto work = [&]() {
+		for (uint32_t i; (i = next.fetch_add(1)) < count;) {
+			const char* lt = ligand_pdbqt[i];
+			const char* ft = flexres_pdbqt ? flexres_pdbqt[i] : nullptr;
+			if (!lt && !ft) { status[i] = ADGPU_ERR_ARG; continue; }
+			adgpu_ligand* l = new (std::nothrow) adgpu_ligand;
+			if (!l) { status[i] = ADGPU_ERR_ARG; continue; }
+			adgpu_status st = prepare_ligand(grid->g, lt ? lt : "", ft ? ft : "", *run, seeds + 3 * (size_t)i, num_runs, l->p);
+			if (st != ADGPU_OK) { delete l; status[i] = st; continue; }
+			out[i] = l;
+			status[i] = ADGPU_OK;
+		}
+	};
+	std::vector<std::thread> pool;
+	for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
+	work();
+	for (auto& t : pool) t.join();
+	for (uint32_t i = 0; i < count; i++)
+		if (status[i] != ADGPU_OK) return fail(status[i], "ligand " + std::to_string(i) + " could not be prepared");
+	return ADGPU_OK;
+}
 
 adgpu_status adgpu_ligand_tables(const adgpu_ligand* lig, adgpu_dockpars* dockpars, adgpu_kc_interintra* interintra,
                                  adgpu_kc_intracontrib* intracontrib, adgpu_kc_intra* intra, adgpu_kc_rotlist* rotlist,

@@ -17,6 +17,8 @@
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <thread>
+#include <atomic>
 #include <string>
 #include <vector>
 #include <algorithm>
@@ -147,20 +149,96 @@ adgpu_status grid_read(const char* fld_path, Grid& g)
 	g.num_map_atypes = (int)g.types.size() - 2;
 	const size_t n = (size_t)g.dims[0] * g.dims[1] * g.dims[2];
 	g.values.assign(n * g.types.size(), 0.0f);
-	std::string dir = dirname_of(fld_path);
-	for (size_t m = 0; m < files.size(); m++) {
-		std::string fn = dir.empty() ? files[m] : dir + "/" + files[m];
-		std::ifstream mf(fn);
-		if (!mf) return fail(ADGPU_ERR_ARG, "cannot open grid map " + fn);
+	const std::string dir = dirname_of(fld_path);
+	// One map per thread: each file is read whole, its lines are cut in place
+	// (newline -> NUL, so every value is parsed from the same text a line
+	// reader would give it) and parsed in order.
+	std::vector<std::string> errors(files.size());
+	auto read_map = [&](size_t m) {
+		const std::string fn = dir.empty() ? files[m] : dir + "/" + files[m];
+		FILE* f = fopen(fn.c_str(), "rb");
+		if (!f) { errors[m] = "cannot open grid map " + fn; return; }
+		std::vector<char> buf;
+		char chunk[1 << 16];
+		size_t got;
+		while ((got = fread(chunk, 1, sizeof(chunk), f)) > 0) buf.insert(buf.end(), chunk, chunk + got);
+		fclose(f);
+		buf.push_back('\0');
+		char* c = buf.data();
+		char* end = c + buf.size() - 1;
+		auto next_line = [&](char*& ln) -> bool {
+			if (c >= end) return false;
+			ln = c;
+			char* nl = static_cast<char*>(memchr(c, '\n', (size_t)(end - c)));
+			if (nl) { *nl = '\0'; c = nl + 1; } else c = end;
+			return true;
+		};
+		char* ln = nullptr;
 		do {
-			if (!std::getline(mf, line)) return fail(ADGPU_ERR_ARG, "grid map preamble too short: " + fn);
-		} while (line.find("CENTER") != 0);
+			if (!next_line(ln)) { errors[m] = "grid map preamble too short: " + fn; return; }
+		} while (strncmp(ln, "CENTER", 6) != 0);
 		float* out = g.values.data() + m * n;
 		for (size_t p = 0; p < n; p++) {
-			if (!std::getline(mf, line)) return fail(ADGPU_ERR_ARG, "grid map too short: " + fn);
-			out[p] = parse_map_value(line.c_str());
+			if (!next_line(ln)) { errors[m] = "grid map too short: " + fn; return; }
+			out[p] = parse_map_value(ln);
 		}
+	};
+	const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+	std::atomic<size_t> next_map(0);
+	std::vector<std::thread> pool;
+	for (unsigned t = 0; t < std::min<size_t>(hw, files.size()); t++)
+		pool.emplace_back([&]() { for (size_t m; (m = next_map.fetch_add(1)) < files.size();) read_map(m); });
+	for (auto& t : pool) t.join();
+	for (auto& e : errors)
+		if (!e.empty()) return fail(ADGPU_ERR_ARG, e);
+	return ADGPU_OK;
+}
+
+// Binary grid cache: "ADGPUGRD", version, dims, spacing, origin, map count,
+// map names (NUL-padded to 8 bytes), then values[map][z][y][x] as float32.
+static const char kGridMagic[8] = {'A', 'D', 'G', 'P', 'U', 'G', 'R', 'D'};
+
+adgpu_status grid_save(const Grid& g, const char* path)
+{
+	FILE* f = fopen(path, "wb");
+	if (!f) return fail(ADGPU_ERR_ARG, std::string("cannot create grid cache ") + path);
+	const int32_t version = 1, nm = (int32_t)g.types.size();
+	bool ok = fwrite(kGridMagic, 1, 8, f) == 8 && fwrite(&version, 4, 1, f) == 1 && fwrite(g.dims, 4, 3, f) == 3 &&
+	          fwrite(&g.spacing, 8, 1, f) == 1 && fwrite(g.origin, 8, 3, f) == 3 && fwrite(&nm, 4, 1, f) == 1;
+	for (int m = 0; ok && m < nm; m++) {
+		char name[8] = {0};
+		strncpy(name, g.types[m].c_str(), 7);
+		ok = fwrite(name, 1, 8, f) == 8;
 	}
+	if (ok) ok = fwrite(g.values.data(), 4, g.values.size(), f) == g.values.size();
+	ok = (fclose(f) == 0) && ok;
+	return ok ? ADGPU_OK : fail(ADGPU_ERR_ARG, std::string("writing grid cache failed: ") + path);
+}
+
+adgpu_status grid_load(const char* path, Grid& g)
+{
+	FILE* f = fopen(path, "rb");
+	if (!f) return fail(ADGPU_ERR_ARG, std::string("cannot open grid cache ") + path);
+	g = Grid();
+	char magic[8];
+	int32_t version = 0, nm = 0;
+	bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, kGridMagic, 8) == 0 && fread(&version, 4, 1, f) == 1 &&
+	          version == 1 && fread(g.dims, 4, 3, f) == 3 && fread(&g.spacing, 8, 1, f) == 1 &&
+	          fread(g.origin, 8, 3, f) == 3 && fread(&nm, 4, 1, f) == 1 && nm >= 3 && nm <= ADGPU_MAX_ATYPES + 2;
+	for (int k = 0; ok && k < 3; k++) ok = g.dims[k] >= 2 && g.dims[k] <= 256;
+	for (int m = 0; ok && m < nm; m++) {
+		char name[9] = {0};
+		ok = fread(name, 1, 8, f) == 8;
+		g.types.push_back(name);
+	}
+	if (ok) {
+		g.values.resize((size_t)g.dims[0] * g.dims[1] * g.dims[2] * nm);
+		ok = fread(g.values.data(), 4, g.values.size(), f) == g.values.size();
+	}
+	fclose(f);
+	if (!ok) return fail(ADGPU_ERR_ARG, std::string("not a valid grid cache: ") + path);
+	if (g.types[nm - 2] != "e" || g.types[nm - 1] != "d") return fail(ADGPU_ERR_ARG, "grid cache: maps must end with e, d");
+	g.num_map_atypes = nm - 2;
 	return ADGPU_OK;
 }
 

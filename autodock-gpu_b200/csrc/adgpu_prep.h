@@ -69,6 +69,8 @@ struct adgpu_ligand_s { adgpu::Prepared p; };
 namespace adgpu {
 
 adgpu_status grid_read(const char* fld_path, Grid& g);
+adgpu_status grid_save(const Grid& g, const char* path);
+adgpu_status grid_load(const char* path, Grid& g);
 void grid_reference_layout(const Grid& g, float* out);      // 4 * nmaps * X*Y*Z floats
 void grid_cell_records(const Grid& g, float* out);          // (X-1)(Y-1)(Z-1) * nmaps * 8 floats
 adgpu_status prepare_ligand(const Grid& grid, const std::string& ligand_text, const std::string& flexres_text,

@@ -298,6 +298,12 @@ adgpu_status adgpu_grid_read(const char* fld_path, adgpu_grid** out);
 adgpu_status adgpu_grid_from_values(const int dims[3], double spacing, const double origin[3], int num_maps,
                                     const char* const* types, const float* values, adgpu_grid** out);
 void adgpu_grid_free(adgpu_grid* grid);
+
+/* Binary grid cache (no reference counterpart; the reference re-reads the
+ * text maps for every job, host/src/processgrid.cpp:186-253): the parsed
+ * maps written once and loaded with one read. */
+adgpu_status adgpu_grid_save(const adgpu_grid* grid, const char* path);
+adgpu_status adgpu_grid_load(const char* path, adgpu_grid** out);
 adgpu_status adgpu_grid_info(const adgpu_grid* grid, int dims[3], double* spacing, double origin[3], int* num_map_atypes);
 
 /* The grid in the reference's device layout (4 floats per point per map,
@@ -318,6 +324,17 @@ adgpu_status adgpu_ligand_prepare(const adgpu_grid* grid, const char* ligand_pdb
                                   const adgpu_dockpars* run, const uint32_t seed[3], int num_runs,
                                   adgpu_ligand** out);
 void adgpu_ligand_free(adgpu_ligand* lig);
+
+/* adgpu_ligand_prepare for `count` ligands on nthreads host threads (0: all
+ * cores); flexres_pdbqt may be NULL (no flexible residues) or hold NULLs;
+ * seeds holds 3 words per ligand.  out[i] / status[i] per ligand; returns the
+ * first failure's status, or ADGPU_OK when every ligand was prepared.  In
+ * the reference each job's setup (files read, tables prepared) runs in the
+ * pipeline thread that then docks it (host/src/main.cpp:303-345). */
+adgpu_status adgpu_ligand_prepare_batch(const adgpu_grid* grid, const char* const* ligand_pdbqt,
+                                        const char* const* flexres_pdbqt, uint32_t count, const adgpu_dockpars* run,
+                                        const uint32_t* seeds, int num_runs, int nthreads, adgpu_ligand** out,
+                                        adgpu_status* status);
 
 /* Copies the prepared tables out (any pointer may be NULL). */
 adgpu_status adgpu_ligand_tables(const adgpu_ligand* lig, adgpu_dockpars* dockpars,

@@ -281,6 +281,17 @@ int adgpu_ref_job_bind(void* h, const void* dockpars_override, uint32_t* prng_st
 
 size_t adgpu_ref_sizeof_refgpudata(void) { return sizeof(RefGpuData); }
 
+/* The reference's own map reading (get_gridinfo + get_gridvalues,
+ * host/src/processgrid.cpp:28-253) of a .maps.fld; returns the number of
+ * floats read (the replicated layout), or -1. */
+long adgpu_ref_read_grid(const char* fld_path)
+{
+	Gridinfo g;
+	if (get_gridinfo(fld_path, &g) != 0) return -1;
+	if (get_gridvalues(&g) != 0) return -1;
+	return (long)g.grids.size();
+}
+
 /* One run's Ligandresult fields (host/inc/processresult.h:40-58). */
 typedef struct {
 	float inter_e, interflex_e, inter_e_elec, intra_e, intraflex_e, rmsd_from_ref, rmsd_from_cluster_center;

@@ -64,6 +64,8 @@ def lib():
         L.adgpu_ref_autostop_free.argtypes = [vp]
         L.adgpu_ref_process_result.argtypes = [vp, vp, vp, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int, vp, vp, vp]
         L.adgpu_ref_rescore.argtypes = [vp, vp, C.c_int, C.c_int, vp]
+        L.adgpu_ref_read_grid.restype = C.c_long
+        L.adgpu_ref_read_grid.argtypes = [C.c_char_p]
         _lib = L
     return _lib
 
