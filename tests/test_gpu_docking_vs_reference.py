@@ -1,0 +1,99 @@
+"""Whole dockings against whole dockings of the reference's own CUDA kernels
+(cuda/*.cu compiled unchanged for sm_100a, oracle/_ref), same ligand, same
+initial population and PRNG seeds, on the same GPU.  Trajectories diverge
+after the first rounding difference, so the comparison is statistical: the
+best energies of the runs come from the same distribution (two-sample
+Kolmogorov-Smirnov), and the top-ranked poses after result processing
+(ordering, re-scoring, RMSD clustering at 2 A) are the same pose: the
+engine's best pose lies within 2 A of the reference's."""
+import ctypes as C
+import json
+
+import numpy as np
+import pytest
+import torch
+
+import helpers
+from adgpu_b200 import device, dock
+from oracle import refpy
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (refpy.cuda_available() and refpy.available()),
+                                 reason="reference CUDA kernels / host oracle not built")]
+T = 64
+LS_ENTRY = {"ad": "gradient_minad", "sw": "perform_ls", "adam": "gradient_minadam"}
+
+
+def reference_docking(case, lsmet, nev, ngen=42000):
+    """docking_with_gpu's generation loop (host/src/performdocking.cpp.Cuda:
+    684-831) over the reference's CUDA kernels: initial population, then GA
+    generation, local search and eval sums until the mean evaluations per
+    run reach nev (check_progress, :908-942)."""
+    dp = case.dockpars
+    R, P, L = case.runs, dp.pop_size, dp.num_of_lsentities
+    job = device.DeviceJob(case.tables, dp, case.grid, R, case.prng)
+    refpy.cuda_lib().adgpu_refcuda_set_gpudata(C.cast(C.pointer(job.g), C.c_void_p))
+    cur, ecur = job.population(case.initpop)
+    nxt, enxt = job.population()
+    refpy.cuda_call("calc_initpop", R * P, T, cur, ecur)
+    refpy.cuda_call("sum_evals", R, T)
+    gens = 0
+    while job.evals_runs.sum().item() / R < nev and gens < ngen:
+        refpy.cuda_call("gen_and_eval_newpops", R * P, T, cur, ecur, nxt, enxt)
+        refpy.cuda_call(LS_ENTRY[lsmet], R * L, T, nxt, enxt)
+        refpy.cuda_call("sum_evals", R, T)
+        gens += 1
+        cur, nxt, ecur, enxt = nxt, cur, enxt, ecur
+    torch.cuda.synchronize()
+    return cur, ecur, gens, job
+
+
+def engine_docking(case, lsmet, nev):
+    dp = case.dockpars
+    job = device.DeviceJob(case.tables, dp, case.grid, case.runs, case.prng)
+    job.activate()
+    r = dock.dock(job, case.initpop, lsmet, nev)
+    torch.cuda.synchronize()
+    return r.conformations, r.energies, r.generations, job
+
+
+def top_pose(case, pops, energies):
+    """The reference's own process_result (host oracle) on a final
+    population: best energy per run, and the best pose of the lowest-energy
+    cluster (cluster 1's centre)."""
+    P = case.info.pop_size
+    p = pops.cpu().numpy().reshape(-1, 64)
+    e = energies.cpu().numpy().reshape(-1)
+    sp, se, runs, xyz, per = case.job.process_result(p, e)
+    best_run = next(i for i, r in enumerate(runs) if r.cluster_id == 1 and r.cluster_subrank == 1)
+    run_best = np.array([r.inter_e + r.intra_e for r in runs], np.float64)
+    return run_best, xyz[best_run], runs[best_run], se.reshape(-1, P)[:, 0]
+
+
+def sym_rmsd(a, b, types):
+    d2 = ((a[:, None, :] - b[None, :, :]) ** 2).sum(-1)
+    d2 = np.where(types[:, None] == types[None, :], d2, np.inf)
+    return float(np.sqrt(d2.min(axis=1).mean()))
+
+
+@pytest.mark.parametrize("lsmet", ["ad", "sw", "adam"])
+def test_docking_matches_reference_cuda_statistically(tmp_path, lsmet):
+    from scipy import stats
+    case = helpers.make_case(str(tmp_path), 40, ["C", "A", "N", "OA", "HD"], 16, 4, 48, config_id=1, lsmet=lsmet)
+    nev = 1_000_000
+    rc, re_, rgen, _ = reference_docking(case, lsmet, nev)
+    ec, ee, egen, _ = engine_docking(case, lsmet, nev)
+    r_best, r_pose, r_top, r_scorer = top_pose(case, rc, re_)
+    e_best, e_pose, e_top, e_scorer = top_pose(case, ec, ee)
+    ks = stats.ks_2samp(e_scorer, r_scorer)
+    N = case.info.true_ligand_atoms
+    types = case.tables["interintra"][1024:2048].view(np.uint32)[:N]
+    d = sym_rmsd(e_pose[:N], r_pose[:N], types)
+    print(json.dumps({"lsmet": lsmet, "generations": [egen, rgen],
+                      "best_energy_median": [float(np.median(e_scorer)), float(np.median(r_scorer))],
+                      "best_energy_min": [float(e_scorer.min()), float(r_scorer.min())], "ks_p": float(ks.pvalue),
+                      "top_pose_rmsd": d,
+                      "top_energy": [float(e_top.inter_e + e_top.intra_e), float(r_top.inter_e + r_top.intra_e)]}))
+    assert abs(egen - rgen) <= max(3, 0.1 * rgen)          # the same evaluation budget spent alike
+    assert ks.pvalue > 1e-3, ks
+    assert d < 2.0, d
