@@ -693,7 +693,17 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 	r->bytes = need;
 	r->natoms = dp.num_of_atoms;
 	r->ntors = dp.num_of_genes - 6;
-	r->tpp = E.cfg.threads_per_pose ? E.cfg.threads_per_pose : tune_tpp(E, *r);
+	if (E.cfg.threads_per_pose) r->tpp = E.cfg.threads_per_pose;
+	else {
+		r->tpp = tune_tpp(E, *r);
+		// Solis-Wets and ADADELTA searches stop on their own test, so every
+		// generation of a run waits for its longest search: two warps per pose
+		// halve that wait, which the steady-state scorer timing cannot see
+		// (64 uneven ligands, nrun 20, ADADELTA: 92.9 k ligands/h at 64 against
+		// 75.2 k with the tuned sizes; serving p50 0.14 s against 0.34 s at 18
+		// requests/s).  ADAM and FIRE run fixed-length searches: tuned size.
+		if ((rp->lsmet == LS_SW || rp->lsmet == LS_AD) && r->tpp < 64) r->tpp = 64;
+	}
 	r->t_submit = now_s();
 	E.used += need;
 	E.stats.submitted++;

@@ -559,7 +559,8 @@ def run_serve(args):
     rate = args.rate if args.rate > 0 else 0.8 * capacity
     arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
     # the serving engine: ticks end on a wall-clock deadline (or a generation count)
-    en = engine.Engine(memory_budget_bytes=budget, gens_per_tick=args.gens_per_tick, tick_ms=args.tick_ms)
+    en = engine.Engine(memory_budget_bytes=budget, gens_per_tick=args.gens_per_tick, tick_ms=args.tick_ms,
+                       threads_per_pose=args.engine_tpp)
     recs = [en.add_receptor(g) for g in grids]
     # serving loop
     t_start = time.perf_counter()
@@ -602,7 +603,7 @@ def run_serve(args):
             "ligands_per_hour": 3600.0 * nreq / t_total, "latency_p50_s": float(np.percentile(lat, 50)),
             "latency_p99_s": float(np.percentile(lat, 99)), "memory_budget_gb": args.budget_gb,
             "gens_per_tick": args.gens_per_tick, "tick_ms": args.tick_ms, "ticks": int(en.stats().ticks),
-            "results_processed_on_device": bool(args.process_results),
+            "results_processed_on_device": bool(args.process_results), "threads_per_pose": args.engine_tpp or "tuned",
             "host_seconds": {"submit": t_submit, "tick": t_tick, "results": t_result, "total": t_total,
                              "engine_kernels": en.stats().kernel_s},
             "worker_utilisation": (en.stats().worker_busy_s / en.stats().worker_span_s
@@ -706,7 +707,7 @@ def main():
     ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel mode)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
     ap.add_argument("--engine-tpp", type=int, default=0,
-                    help="engine threads per pose (batch mode): 0 = autotuned per ligand size, or 32, 64, 128")
+                    help="engine threads per pose (batch / serve modes): 0 = autotuned per ligand size, or 32, 64, 128")
     ap.add_argument("--nlig", type=int, default=64, help="ligands (batch mode)")
     ap.add_argument("--batch-config", type=int, default=3, choices=[3, 4],
                     help="batch mode workload: 3 (uneven ligands) or 4 (80^3 maps, 2 flexible residues, nrun 50)")
