@@ -700,8 +700,11 @@ adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_ref
                                   double* best_xyz, float* peratom, float* entities)
 {
 	if (!lig) return fail(ADGPU_ERR_ARG, "null argument");
+	// a blocking stream: ordered after the caller's work on the legacy
+	// default stream (where the kernel API and torch's default stream write
+	// the final populations)
 	cudaStream_t st = nullptr;
-	cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+	cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamDefault);
 	if (e != cudaSuccess) return cuda_fail(e, "stream");
 	adgpu_status rc = process_result_core(lig->p.post, lig->p.pairs.data(), lig->p.dockpars, grid_reference_layout, 0,
 	                                      populations, energies, num_runs, params, runs_out, clusters_out, num_clusters,
