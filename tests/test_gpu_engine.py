@@ -52,21 +52,22 @@ def test_engine_matches_plain_path(grid, lsmet, monkeypatch):
     np.testing.assert_array_equal(r.best_energies, e_plain.min(axis=1))
 
 
-def test_batch_uneven_ligands_and_mix_invariance(grid):
+@pytest.mark.parametrize("tpp", [32, 64])
+def test_batch_uneven_ligands_and_mix_invariance(grid, tpp):
     sizes = [(12, 0), (16, 4), (24, 8), (30, 12), (20, 6), (40, 16)]
     ligs = [ligand(grid, i, a, t, runs=3) for i, (a, t) in enumerate(sizes)]
     nev = 40_000
     # alone
     alone = []
     for lg in ligs[:3]:
-        en = engine.Engine(threads_per_pose=32)
+        en = engine.Engine(threads_per_pose=tpp)
         rec = en.add_receptor(grid)
         rid = en.submit(lg, rec, "ad", max_evals=nev)
         en.run()
         alone.append(en.result(rid))
         en.close()
     # all together in one batch
-    en = engine.Engine(threads_per_pose=32)
+    en = engine.Engine(threads_per_pose=tpp)
     rec = en.add_receptor(grid)
     ids = [en.submit(lg, rec, "ad", max_evals=nev) for lg in ligs]
     en.run()
@@ -80,6 +81,23 @@ def test_batch_uneven_ligands_and_mix_invariance(grid):
         e0 = np.array([lg.initpop.shape[0]])  # noqa: F841
         assert np.all(np.isfinite(r.best_energies))
         assert r.best_energies.max() < 1e6
+
+
+def test_automatic_threads_per_pose(grid):
+    """Without a configured size: the tuned size per ligand-size bucket, at
+    least 64 for the searches that stop on their own test (Solis-Wets,
+    ADADELTA), whose phases wait for their longest search."""
+    en = engine.Engine()
+    rec = en.add_receptor(grid)
+    lg = ligand(grid, 3, 20, 6, runs=2)
+    got = {}
+    for m in ("sw", "ad", "adam", "fire"):
+        rid = en.submit(lg, rec, m, max_evals=5_000)
+        got[m] = en.info(rid)[0]
+    en.run()
+    assert got["sw"] >= 64 and got["ad"] >= 64
+    assert all(v in (32, 64, 128) for v in got.values())
+    en.close()
 
 
 def test_continuous_admission_and_budget(grid):
