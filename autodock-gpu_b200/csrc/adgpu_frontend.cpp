@@ -129,6 +129,7 @@ adgpu_status adgpu_ligand_prepare_batch(const adgpu_grid* grid, const char* cons
 	unsigned nt = nthreads > 0 ? (unsigned)nthreads : hw;
 	nt = std::max(1u, std::min<unsigned>(nt, count));
 	std::atomic<uint32_t> next(0);
+	std::vector<std::string> why(count);     // a worker's error text (the last error is per thread)
 	auto work = [&]() {
 		for (uint32_t i; (i = next.fetch_add(1)) < count;) {
 			const char* lt = ligand_pdbqt[i];
@@ -137,7 +138,7 @@ adgpu_status adgpu_ligand_prepare_batch(const adgpu_grid* grid, const char* cons
 			adgpu_ligand* l = new (std::nothrow) adgpu_ligand;
 			if (!l) { status[i] = ADGPU_ERR_ARG; continue; }
 			adgpu_status st = prepare_ligand(grid->g, lt ? lt : "", ft ? ft : "", *run, seeds + 3 * (size_t)i, num_runs, l->p);
-			if (st != ADGPU_OK) { delete l; status[i] = st; continue; }
+			if (st != ADGPU_OK) { delete l; status[i] = st; why[i] = adgpu_last_error(); continue; }
 			out[i] = l;
 			status[i] = ADGPU_OK;
 		}
@@ -147,7 +148,9 @@ adgpu_status adgpu_ligand_prepare_batch(const adgpu_grid* grid, const char* cons
 	work();
 	for (auto& t : pool) t.join();
 	for (uint32_t i = 0; i < count; i++)
-		if (status[i] != ADGPU_OK) return fail(status[i], "ligand " + std::to_string(i) + " could not be prepared");
+		if (status[i] != ADGPU_OK)
+			return fail(status[i], "ligand " + std::to_string(i) + " could not be prepared" +
+			                           (why[i].empty() ? std::string() : ": " + why[i]));
 	return ADGPU_OK;
 }
 
