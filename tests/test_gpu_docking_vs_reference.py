@@ -76,10 +76,15 @@ def sym_rmsd(a, b, types):
     return float(np.sqrt(d2.min(axis=1).mean()))
 
 
-@pytest.mark.parametrize("lsmet", ["ad", "sw", "adam"])
-def test_docking_matches_reference_cuda_statistically(tmp_path, lsmet):
+@pytest.mark.parametrize("lsmet,size", [("ad", "cfg1"), ("sw", "cfg1"), ("adam", "cfg1"), ("ad", "cfg2")])
+def test_docking_matches_reference_cuda_statistically(tmp_path, lsmet, size):
+    """cfg1: 16 heavy atoms / 4 torsions on 40^3 maps; cfg2: the benchmark's
+    ligand, 40 heavy atoms / 10 torsions on 60^3 maps."""
     from scipy import stats
-    case = helpers.make_case(str(tmp_path), 40, ["C", "A", "N", "OA", "HD"], 16, 4, 48, config_id=1, lsmet=lsmet)
+    if size == "cfg1":
+        case = helpers.make_case(str(tmp_path), 40, ["C", "A", "N", "OA", "HD"], 16, 4, 48, config_id=1, lsmet=lsmet)
+    else:
+        case = helpers.make_case(str(tmp_path), 60, ["C", "A", "N", "OA", "HD"], 40, 10, 48, config_id=2, lsmet=lsmet)
     nev = 1_000_000
     rc, re_, rgen, _ = reference_docking(case, lsmet, nev)
     ec, ee, egen, _ = engine_docking(case, lsmet, nev)
@@ -89,7 +94,7 @@ def test_docking_matches_reference_cuda_statistically(tmp_path, lsmet):
     N = case.info.true_ligand_atoms
     types = case.tables["interintra"][1024:2048].view(np.uint32)[:N]
     d = sym_rmsd(e_pose[:N], r_pose[:N], types)
-    print(json.dumps({"lsmet": lsmet, "generations": [egen, rgen],
+    print(json.dumps({"lsmet": lsmet, "size": size, "generations": [egen, rgen],
                       "best_energy_median": [float(np.median(e_scorer)), float(np.median(r_scorer))],
                       "best_energy_min": [float(e_scorer.min()), float(r_scorer.min())], "ks_p": float(ks.pvalue),
                       "top_pose_rmsd": d,
