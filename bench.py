@@ -395,11 +395,29 @@ def run_engine(args, rank, world, local_rank):
                 "clocks": clocks, "roofline": roof, "cost_model": cm}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(lig, args.lsmet)
+        # the single-GPU samples below run at N = 1 only (under torchrun the
+        # other ranks would wait for them at the closing barrier)
+        if world > 1:
+            args.no_batch = args.no_serve = args.no_result = True
         if not args.no_batch:
             # the batching comparison on a bounded sample of its configuration
             bvp = run_batch(args)
             line["batched_vs_plain"] = {k: bvp[k] for k in ("ligands", "nrun", "nev_per_run", "heavy_atoms", "batched",
                                                             "plain", "batched_over_plain_ligands_per_hour", "tpp_classes")}
+        if not args.no_serve:
+            # the serving loop on a shorter request stream (same settings as --mode serve)
+            sargs = argparse.Namespace(**vars(args))
+            sargs.nreq = 100
+            sargs.process_results = True
+            sv = run_serve(sargs)
+            line["serving"] = {k: sv[k] for k in ("requests", "nrun", "nev_per_run", "receptors",
+                                                  "batched_capacity_ligands_per_s", "arrival_rate_per_s",
+                                                  "ligands_per_hour", "latency_p50_s", "latency_p99_s", "tick_ms",
+                                                  "results_processed_on_device")}
+        if not args.no_result:
+            rr = run_result(args)
+            line["result_processing"] = {k: rr[k] for k in ("workload", "gpu_ms_all_entities", "reference_host_ms",
+                                                            "speedup_vs_reference", "clusters", "parity")}
         del evals_per_docking
     return line
 
@@ -703,6 +721,8 @@ def main():
     ap.add_argument("--lsmet", default="ad", choices=["ad", "sw", "adam", "fire"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain sample in the default mode")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving sample in the default mode")
+    ap.add_argument("--no-result", action="store_true", help="skip the result-processing sample in the default mode")
     ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel", "batch", "serve", "result"])
     ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel mode)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
