@@ -5,6 +5,7 @@
 #include <cstring>
 #include <algorithm>
 #include "adgpu_tables.h"
+#include <vector>
 
 namespace adgpu {
 
@@ -25,6 +26,64 @@ static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 size_t cell_grid_bytes(int gx, int gy, int gz, int num_map_atypes)
 {
 	return (size_t)(gx - 1) * (gy - 1) * (gz - 1) * (size_t)(num_map_atypes + 2) * 8 * sizeof(float);
+}
+
+// Pair order for the scorer's force atomics.  One warp instruction handles an
+// aligned group of 32 consecutive pairs, and its atomics take one
+// shared-memory pass per pair that shares a bank (atom index mod 32) with
+// another pair of the group on the same side.  The pairs, sorted by the banks
+// of their atoms, are dealt round-robin over the groups, which spreads every
+// bank's pairs evenly; then each group flips pairs while that lowers the
+// larger bank count of its first-atom side plus that of its second-atom side.
+// A pair's energy and force do not depend on its orientation: the record
+// fields are computed from its original order and the force update is
+// antisymmetric (x1 - x2 = -(x2 - x1), symmetric fixed-point rounding), so
+// only the order of the per-thread energy sums changes.
+static void order_pairs(const uint32_t* pairs, int Q, std::vector<uint32_t>& pos, std::vector<uint8_t>& swapped)
+{
+	pos.assign(Q, 0);
+	swapped.assign(Q, 0);
+	if (Q == 0) return;
+	std::vector<int> idx(Q);
+	for (int p = 0; p < Q; p++) idx[p] = p;
+	std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+		const uint32_t ka = ((pairs[2 * a] & 31) << 5) | (pairs[2 * a + 1] & 31);
+		const uint32_t kb = ((pairs[2 * b] & 31) << 5) | (pairs[2 * b + 1] & 31);
+		return ka < kb;
+	});
+	const int G = (Q + 31) / 32;
+	std::vector<std::vector<int>> groups(G);
+	int g = 0;
+	for (int p : idx) {
+		while ((int)groups[g].size() >= (g == G - 1 ? Q - 32 * (G - 1) : 32)) g = (g + 1) % G;
+		groups[g].push_back(p);
+		g = (g + 1) % G;
+	}
+	auto cost = [&](const std::vector<int>& grp) {
+		int c1[32] = {0}, c2[32] = {0}, m1 = 0, m2 = 0;
+		for (int p : grp) {
+			const int a = (int)(pairs[2 * p] & 31), b = (int)(pairs[2 * p + 1] & 31);
+			const int f = swapped[p] ? b : a, s2 = swapped[p] ? a : b;
+			m1 = std::max(m1, ++c1[f]);
+			m2 = std::max(m2, ++c2[s2]);
+		}
+		return m1 + m2;
+	};
+	for (int gi = 0; gi < G; gi++) {
+		std::vector<int>& grp = groups[gi];
+		int best = cost(grp);
+		for (int pass = 0; pass < 4; pass++) {
+			bool improved = false;
+			for (int p : grp) {
+				swapped[p] ^= 1;
+				const int c = cost(grp);
+				if (c < best) { best = c; improved = true; }
+				else swapped[p] ^= 1;
+			}
+			if (!improved) break;
+		}
+		for (size_t k = 0; k < grp.size(); k++) pos[grp[k]] = (uint32_t)(32 * gi + k);
+	}
 }
 
 adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii, const uint32_t* pairs,
@@ -119,11 +178,15 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 		mv[k] = make_float4(cf.rotbonds_moving_vectors_const[3 * k], cf.rotbonds_moving_vectors_const[3 * k + 1], cf.rotbonds_moving_vectors_const[3 * k + 2], 0.f);
 		ends[k] = make_int2(rotbonds[2 * k], rotbonds[2 * k + 1]);
 	}
-	// pairs and torsion items in warp-interleaved order (interleave_pos)
+	// torsion items in warp-interleaved order (interleave_pos), pairs in
+	// bank-spread groups of 32 (order_pairs)
 	uint32_t* it_out = reinterpret_cast<uint32_t*>(B + out.off_tor_items);
 	for (size_t i = 0; i < items.size(); i++) it_out[interleave_pos((uint32_t)i, (uint32_t)items.size())] = items[i];
 	PairRec* pr = reinterpret_cast<PairRec*>(B + out.off_pairs);
 	const int nat = dp.num_of_atypes;
+	std::vector<uint32_t> ppos;
+	std::vector<uint8_t> pswap;
+	order_pairs(pairs, Q, ppos, pswap);
 	for (int p = 0; p < Q; p++) {
 		uint32_t a1 = pairs[2 * p], a2 = pairs[2 * p + 1];
 		if (a1 >= (uint32_t)N || a2 >= (uint32_t)N) return fail(ADGPU_ERR_ARG, "intramolecular pair atom out of range");
@@ -143,9 +206,9 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 		               (kin.dspars_S_const[t2] + dp.qasp * std::fabs(q2)) * kin.dspars_V_const[t1];
 		r.qq = dp.coeff_elec * q1 * q2;
 		r.vbond = cgg0 ? 50.0f : 0.0f;
-		r.ij = a1 | (a2 << 8) | (m << 16) | (n << 24);
+		r.ij = (pswap[p] ? (a2 | (a1 << 8)) : (a1 | (a2 << 8))) | (m << 16) | (n << 24);
 		r.pad = 0;
-		pr[interleave_pos((uint32_t)p, (uint32_t)Q)] = r;
+		pr[ppos[p]] = r;
 	}
 	return ADGPU_OK;
 }
