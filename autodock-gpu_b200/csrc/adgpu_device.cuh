@@ -49,8 +49,8 @@ struct __align__(16) PairRec {
 	uint32_t pad;
 };
 
-// Stored position of element p of a list of n (pairs, torsion items) in
-// warp-interleaved order.  The reference lists pairs by first atom and items
+// Stored position of element p of a list of n (torsion items; pairs in the
+// kernel-API repack of adgpu_noalloc.cu) in warp-interleaved order.  The reference lists pairs by first atom and items
 // by torsion, so 32 consecutive entries mostly share an atom or a torsion and
 // a warp's shared-memory gradient atomics on it would serialise.  The list is
 // cut into up to 32 consecutive stretches of K entries and stored row by row:
