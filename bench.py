@@ -362,11 +362,14 @@ def run_engine(args, rank, world, local_rank):
         import ctypes as C
         peak = C.c_float(0)
         lib.call("adgpu_measure_fp32_peak", scratch, scratch.numel(), C.byref(peak))
-        traffic = None
+        traffic = issue = instr = None
         tfile = os.path.join(ROOT, "profiles", "ls_kernel_traffic.json")
         if os.path.exists(tfile):
             try:
-                traffic = json.load(open(tfile)).get(args.lsmet)
+                prof = json.load(open(tfile))
+                traffic = prof.get(args.lsmet)
+                issue = prof.get(f"{args.lsmet}_issue_active")
+                instr = prof.get(f"{args.lsmet}_warp_instructions_per_eval")
             except Exception:
                 traffic = None
         roof = {"bound": "fp32", "achieved": achieved, "peak": float(peak.value), "unit": "TFLOP/s",
@@ -374,6 +377,9 @@ def run_engine(args, rank, world, local_rank):
                 "traffic_source": "ncu dram bytes per launch of this launch shape (profiles/ls_kernel_traffic.json)",
                 "peak_source": "measured in this run (FMA-chain probe, adgpu_measure_fp32_peak); "
                                "MEASURED_PEAKS.json has no FP32 figure",
+                # the kernel is bound by instruction issue, not by a pipe: the
+                # share of issue slots it uses (ncu, same launch shape)
+                "issue_slots_active": issue, "warp_instructions_per_eval": instr,
                 "kernel": entry, "launch_ms": dur * 1e3, "evals_per_launch": statistics.mean(ls_evals),
                 "flop_per_eval": flop_per_eval, "bytes_per_eval": cm["bytes"],
                 "hbm_frac_of_measured": (statistics.mean(ls_evals) * cm["bytes"] / dur / 1e9) / _hbm_peak()}
