@@ -87,3 +87,16 @@ def score(genotypes: np.ndarray, gradients: bool, device="cuda:0"):
     lib.call("adgpu_score_genotypes", n, g, e, gr if gr is not None else None)
     torch.cuda.synchronize()
     return (e.cpu().numpy(), gr.cpu().numpy()) if gradients else e.cpu().numpy()
+
+
+def score_terms(genotypes: np.ndarray, device="cuda:0"):
+    """Energies and their eight terms per genotype (adgpu_score_terms): inter
+    type / elec / desolv, intra vdW-Hb / elec / desolv / CG-G0, atoms outside
+    the grid."""
+    g = torch.from_numpy(np.ascontiguousarray(genotypes, np.float32)).to(device)
+    n = g.shape[0]
+    e = torch.zeros(n, dtype=torch.float32, device=device)
+    t = torch.zeros((n, 8), dtype=torch.float32, device=device)
+    lib.call("adgpu_score_terms", n, g, e, t)
+    torch.cuda.synchronize()
+    return e.cpu().numpy(), t.cpu().numpy()

@@ -28,6 +28,7 @@ SIGNATURES = {
     "adgpu_gradient_minadam": (_i, [_u32, _u32, _vp, _vp]),
     "adgpu_gradient_minfire": (_i, [_u32, _u32, _vp, _vp]),
     "adgpu_score_genotypes": (_i, [_u32, _vp, _vp, _vp]),
+    "adgpu_score_terms": (_i, [_u32, _vp, _vp, _vp]),
     "adgpu_score_genotypes_noalloc": (_i, [_vp, _u32, _vp, _vp, _vp]),
     "adgpu_dock_resident": (_i, [_i, _u32, _u64, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
     "adgpu_dock_resident_autostop": (_i, [_i, _u32, _u64, _u32, _u32, C.c_float, _u64,

@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(128, ADGPU_MIN_CTAS) lga_kernel(KArgs a, float
 		else if constexpr (KIND == 5) initpop_block<TPP>(a, b, G, S);
 		else if constexpr (KIND == 6) score_block<TPP, false>(a, b, G, S, grads);
 		else if constexpr (KIND == 7) score_block<TPP, true>(a, b, G, S, grads);
+		else if constexpr (KIND == 8) score_terms_block<TPP>(a, b, G, S, grads);
 	}
 }
 
@@ -454,6 +455,7 @@ static adgpu_status run_kind(int kind, uint32_t blocks, uint32_t threads, const 
 	case 5: st = launch_kind<5>(a, grads, 0, s.tpp); break;
 	case 6: st = launch_kind<6>(a, grads, 0, s.tpp); break;
 	case 7: st = launch_kind<7>(a, grads, 0, s.tpp); break;
+	case 8: st = launch_kind<8>(a, grads, 0, s.tpp); break;
 	default: return fail(ADGPU_ERR_ARG, "bad kernel kind");
 	}
 	if (st != ADGPU_OK) return st;
@@ -509,6 +511,12 @@ adgpu_status adgpu_gradient_minfire(uint32_t blocks, uint32_t threads, float* cn
 adgpu_status adgpu_score_genotypes(uint32_t n, const float* genotypes, float* energies, float* gradients)
 {
 	return run_kind(gradients ? 7 : 6, n, 64, nullptr, nullptr, const_cast<float*>(genotypes), energies, gradients);
+}
+
+adgpu_status adgpu_score_terms(uint32_t n, const float* genotypes, float* energies, float* terms)
+{
+	if (!genotypes || !energies || !terms) return fail(ADGPU_ERR_ARG, "null buffer");
+	return run_kind(8, n, 64, nullptr, nullptr, const_cast<float*>(genotypes), energies, terms);
 }
 
 adgpu_status adgpu_dock_resident(int lsmet, uint32_t num_runs, uint64_t max_evals, uint32_t max_gens,

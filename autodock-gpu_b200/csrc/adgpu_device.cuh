@@ -312,8 +312,10 @@ static __device__ __noinline__ float pow_int(float b, int e)
 // are the reference's (cuda/calcMergeEneGra.cu:418-602) rewritten with one
 // reciprocal square root and three reciprocals per pair instead of divisions
 // and __powf:  (AC - sd^(m-n) BD) sd^-m = AC/sd^m - BD/sd^n  (m = 12, n = 6 or 10).
-template <int TPP, bool GRAD>
-__device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, int rank)
+// TERMS (energy only): also adds this thread's vdW/H-bond, electrostatic,
+// desolvation and CG-G0 sums to tsum[0..3].
+template <int TPP, bool GRAD, bool TERMS = false>
+__device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, int rank, float* tsum = nullptr)
 {
 	constexpr uint32_t k12_6 = 12u | (6u << 8), k12_10 = 12u | (10u << 8);
 	// loop invariants read once: when L lives in shared memory (the engine's
@@ -325,6 +327,7 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 	const PairRec* const pairs = L.pairs;
 	const float spacing = L.spacing, inv_spacing = L.inv_spacing, coeff_desolv = L.coeff_desolv;
 	float2 esum = f2s(0.0f);
+	float2 t_vdw = f2s(0.0f), t_el = f2s(0.0f), t_ds = f2s(0.0f), t_cg = f2s(0.0f);
 	for (int p = rank; p < npairs; p += 2 * TPP) {
 		const bool has_b = p + TPP < npairs;          // the second pair; else pair a twice, b discarded
 		const float4* pra = reinterpret_cast<const float4*>(pairs + p);
@@ -343,6 +346,7 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 		const float2 vbond = f2(Ba.y, Bb.y);          // G for CG-G0 pairs, else 0
 		float2 e = f2mul(vbond, r);
 		float2 pg = vbond;
+		if constexpr (TERMS) t_cg = f2add(t_cg, f2mul(f2(1.0f, has_b ? 1.0f : 0.0f), f2mul(vbond, r)));
 		// vdW / H-bond, cut-off 8 A
 		{
 			const float2 reqm = f2(Aa.z, Ab.z);
@@ -373,6 +377,7 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 			// cut-off as a 0/1 factor: the terms are finite for every r (sd >= r - hs)
 			const float2 in8 = f2(lt1(r.x, 8.0f), lt1(r.y, 8.0f));
 			e = f2fma(in8, ev, e);
+			if constexpr (TERMS) t_vdw = f2add(t_vdw, f2mul(f2(1.0f, has_b ? 1.0f : 0.0f), f2mul(in8, ev)));
 			if (GRAD) {
 				const float2 gv = f2mul(f2add(f2mul(fn, bd_in), f2neg(f2mul(fm, ac_im))), inv);
 				pg = f2fma(in8, gv, pg);
@@ -396,6 +401,11 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 			const float2 es = f2mul(f2(Ba.x, Bb.x), inv_r);
 			const float2 ee = f2fma(diel, es, desolv);
 			e = f2fma(in20, ee, e);
+			if constexpr (TERMS) {
+				const float2 bm = f2(1.0f, has_b ? 1.0f : 0.0f);
+				t_el = f2add(t_el, f2mul(bm, f2mul(in20, f2mul(diel, es))));
+				t_ds = f2add(t_ds, f2mul(bm, f2mul(in20, desolv)));
+			}
 			if (GRAD) {
 				const float2 t1 = f2mul(f2mul(es, inv_r), diel);
 				const float2 t2 = f2mul(f2mul(f2mul(es, f2s(2.21718f)), rs2), rs);
@@ -420,6 +430,12 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 			}
 		}
 	}
+	if constexpr (TERMS) {
+		tsum[0] += t_vdw.x + t_vdw.y;
+		tsum[1] += t_el.x + t_el.y;
+		tsum[2] += t_ds.x + t_ds.y;
+		tsum[3] += t_cg.x + t_cg.y;
+	}
 	return esum.x + esum.y;
 }
 
@@ -430,9 +446,13 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 // REF_GRID: L.grid is the reference's own layout (4 replicated floats per
 // point and map, host/src/processgrid.cpp:244-248) instead of cell records;
 // the same 8 corner values are read, from two 16-byte loads per map.
-template <int TPP, bool GRAD, bool REF_GRID = false>
+// TERMS (energy only): terms[0..7] (written by rank 0) = intermolecular type
+// map, electrostatic and desolvation energies, intramolecular vdW/H-bond,
+// electrostatic, desolvation and CG-G0 energies, and the number of atoms
+// outside the grid.
+template <int TPP, bool GRAD, bool REF_GRID = false, bool TERMS = false>
 __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float* __restrict__ grad,
-                           const PoseSmem& S, const Group<TPP>& G)
+                           const PoseSmem& S, const Group<TPP>& G, float* terms = nullptr)
 {
 	const int rank = G.rank;
 	// 1. torsion quaternions (cuda/calcMergeEneGra.cu:160-175, computed once per
@@ -462,6 +482,7 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	//    (the per-atom order the reference's rotation list encodes, cuda/calcMergeEneGra.cu:131-190);
 	//    the same thread then takes the atom's intermolecular terms (3.)
 	float e_acc = 0.0f;
+	float tt[TERMS ? 8 : 1] = {0.f};   // TERMS partial sums
 	for (int a = rank; a < L.natoms; a += TPP) {
 		float4 r4 = L.atom_xyzq[a];
 		float3 p = make_float3(r4.x, r4.y, r4.z);
@@ -490,6 +511,7 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 			if (x < 0.f || y < 0.f || z < 0.f || x >= (float)(L.gx - 1) || y >= (float)(L.gy - 1) || z >= (float)(L.gz - 1)) {
 				e_acc += kOutOfGridPenalty;
 				fx = fy = fz = kOutOfGridForce;
+				if constexpr (TERMS) tt[7] += 1.0f;
 			} else {
 				float xl = floorf(x), yl = floorf(y), zl = floorf(z);
 				float dx = x - xl, omdx = 1.0f - dx, dy = y - yl, omdy = 1.0f - dy, dz = z - zl, omdz = 1.0f - dz;
@@ -518,6 +540,7 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 				e_acc += vt;
 				e_acc += q * ve;
 				e_acc += fabsf(q) * vd;
+				if constexpr (TERMS) { tt[0] += vt; tt[1] += q * ve; tt[2] += fabsf(q) * vd; }
 				if (GRAD) {
 					// corners: .x .y .z .w of rec0 = 000 010 001 011 ; of rec1 = 100 110 101 111
 #define ADGPU_GX(c0, c1) (omdz * (omdy * (c1.x - c0.x) + dy * (c1.y - c0.y)) + dz * (omdy * (c1.z - c0.z) + dy * (c1.w - c0.w)))
@@ -541,7 +564,13 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	G.sync();
 
 	// 4. intramolecular pairs (cuda/calcMergeEneGra.cu:418-602)
-	e_acc += pair_terms<TPP, GRAD>(L, S, rank);
+	if constexpr (TERMS) e_acc += pair_terms<TPP, GRAD, TERMS>(L, S, rank, tt + 3);
+	else e_acc += pair_terms<TPP, GRAD>(L, S, rank);
+	if constexpr (TERMS) {
+		G.template sum_n<8>(tt);
+		if (rank == 0)
+			for (int k = 0; k < 8; k++) terms[k] = tt[k];
+	}
 	if (!GRAD) return G.sum(e_acc);
 	G.sync();   // every pair's forces are in S.fx/fy/fz
 

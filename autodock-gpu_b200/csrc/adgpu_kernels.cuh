@@ -469,4 +469,17 @@ __device__ void score_block(const KArgs& a, uint32_t b, const Group<TPP>& G, con
 	G.sync();
 }
 
+// The scorer's energy terms (energy only) of nblocks genotypes: a.e[b] the
+// energy, out[8b .. 8b+7] the terms (score_pose with TERMS).
+template <int TPP>
+__device__ void score_terms_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S, float* out)
+{
+	const int NG = a.dp.num_of_genes;
+	for (int k = G.rank; k < NG; k += TPP) S.gen[k] = a.conf[(size_t)b * kGenotypeStride + k];
+	G.sync();
+	const float e = score_pose<TPP, false, false, true>(a.L, S.gen, S.grad, S.pose, G, out + (size_t)b * 8);
+	if (G.rank == 0) a.e[b] = e;
+	G.sync();
+}
+
 }  // namespace adgpu

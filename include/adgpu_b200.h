@@ -243,6 +243,14 @@ adgpu_status adgpu_score_genotypes(uint32_t n, const float* genotypes,
  * calls that overlap on the GPU (from several host threads) race on it.
  * Runs on the legacy default stream and returns after the scores are
  * written. */
+/* The scorer's energy split into its terms, for n genotypes (device
+ * buffers; no reference counterpart, the parity tests' per-term view):
+ * energies[n], and terms[8n] per genotype = intermolecular type-map,
+ * electrostatic and desolvation energies, intramolecular vdW/H-bond,
+ * electrostatic, desolvation and CG-G0 energies, and the number of atoms
+ * outside the grid (each adds the 2^24 penalty to the energy only). */
+adgpu_status adgpu_score_terms(uint32_t n, const float* genotypes, float* energies, float* terms);
+
 adgpu_status adgpu_score_genotypes_noalloc(const adgpu_gpudata* data, uint32_t n,
                                            const float* genotypes, float* energies,
                                            float* gradients);

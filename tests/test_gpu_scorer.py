@@ -100,3 +100,25 @@ def test_maximum_size_parity(tmp_path):
     ng = case.ngenes
     assert np.all(np.abs(gr_gpu[:, :ng] - gr_ref[:, :ng]) <= helpers.gradient_bound(case, gr_ref))
     del dj
+
+
+@pytest.mark.parametrize("name", ["cfg1", "cfg2", "flex"])
+def test_per_term_energies(cases, name):
+    """Each energy term against the oracle's, for identical genotypes: the
+    three intermolecular maps and the four intramolecular terms, each within
+    1e-4 relative plus a floor of 1e-6 of the pose's summed |terms| (the
+    oracle sums in another order); the out-of-grid count exactly."""
+    from adgpu_b200 import device
+    case = cases[name]
+    _activate(case)
+    g = helpers.in_box_genotypes(case, 400, seed=17)
+    g[:20, 0] = -3.0                      # some atoms outside the grid
+    e, t = device.score_terms(g)
+    ref = np.array([case.host.score_terms(x)[2] for x in g])
+    assert np.array_equal(t[:, 7], ref[:, 7])
+    scale = np.abs(ref[:, :7]).sum(axis=1, keepdims=True)
+    tol = 1e-4 * np.abs(ref[:, :7]) + 1e-6 * scale + 1e-5
+    assert np.all(np.abs(t[:, :7] - ref[:, :7]) <= tol), np.abs(t[:, :7] - ref[:, :7]).max(axis=0)
+    # the terms add up to the energy (plus the out-of-grid penalties)
+    total = t[:, :7].astype(np.float64).sum(axis=1) + 16777216.0 * t[:, 7]
+    assert np.allclose(total, e, rtol=1e-5, atol=1e-3)
