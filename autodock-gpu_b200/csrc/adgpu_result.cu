@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 #include "adgpu_prep.h"
 #include "adgpu_result.h"
@@ -706,9 +707,32 @@ adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_ref
 	cudaStream_t st = nullptr;
 	cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamDefault);
 	if (e != cudaSuccess) return cuda_fail(e, "stream");
+	// scratch from a pool of this library that keeps its memory between calls
+	// (one per device), so repeated calls do not go back to the driver
+	static std::mutex pool_mu;
+	static cudaMemPool_t pools[64] = {};
+	cudaMemPool_t pool = nullptr;
+	int dev = 0;
+	if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
+		std::lock_guard<std::mutex> lk(pool_mu);
+		if (!pools[dev]) {
+			cudaMemPoolProps props{};
+			props.allocType = cudaMemAllocationTypePinned;
+			props.location.type = cudaMemLocationTypeDevice;
+			props.location.id = dev;
+			if (cudaMemPoolCreate(&pools[dev], &props) == cudaSuccess) {
+				uint64_t keep = 256ull << 20;
+				cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+			} else {
+				pools[dev] = nullptr;
+				cudaGetLastError();
+			}
+		}
+		pool = pools[dev];
+	}
 	adgpu_status rc = process_result_core(lig->p.post, lig->p.pairs.data(), lig->p.dockpars, grid_reference_layout, 0,
 	                                      populations, energies, num_runs, params, runs_out, clusters_out, num_clusters,
-	                                      best_xyz, peratom, entities, st, nullptr);
+	                                      best_xyz, peratom, entities, st, pool);
 	cudaStreamDestroy(st);
 	return rc;
 }
