@@ -733,7 +733,8 @@ def main():
     ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel mode)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
     ap.add_argument("--engine-tpp", type=int, default=0,
-                    help="engine threads per pose (batch / serve modes): 0 = autotuned per ligand size, or 32, 64, 128")
+                    help="engine threads per pose (batch / serve modes): 0 = automatic (tuned per ligand size, "
+                         "at least 64 for sw/ad), or 32, 64, 128")
     ap.add_argument("--nlig", type=int, default=64, help="ligands (batch mode)")
     ap.add_argument("--batch-config", type=int, default=3, choices=[3, 4],
                     help="batch mode workload: 3 (uneven ligands) or 4 (80^3 maps, 2 flexible residues, nrun 50)")
