@@ -130,3 +130,16 @@ def table_offsets():
 
 def as_bytes_array(x) -> np.ndarray:
     return np.frombuffer(bytes(x), dtype=np.uint8).copy()
+
+
+class DockStats(C.Structure):
+    """adgpu_dock_stats: accounting of the last adgpu_dock_resident call."""
+    _fields_ = [("pipelined", C.c_int), ("threads_per_pose", C.c_int), ("pose_groups", C.c_int),
+                ("generations", C.c_uint32), ("generations_discarded", C.c_uint32), ("tasks", C.c_uint64),
+                ("parks", C.c_uint64), ("busy_s", C.c_double), ("span_s", C.c_double)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        if self.pipelined and self.pose_groups and self.span_s > 0:
+            d["utilisation"] = self.busy_s / (self.pose_groups * self.span_s)
+        return d

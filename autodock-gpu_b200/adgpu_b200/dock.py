@@ -105,3 +105,12 @@ def dock(job: DeviceJob, initpop: np.ndarray | torch.Tensor, lsmet: str = "ad", 
                  C.byref(stopped))
     c, e = (c2, e2) if fin.value else (c1, e1)
     return DockResult(c, e, job.evals_runs.cpu().numpy().copy(), gens.value, bool(stopped.value))
+
+
+def last_stats() -> dict:
+    """Accounting of the last docking through adgpu_dock_resident: whether the
+    pipelined loop ran, its pose groups, tasks, their summed busy time, the
+    launch span and the resulting utilisation of the pose groups."""
+    st = abi.DockStats()
+    lib.call("adgpu_dock_stats_get", C.byref(st))
+    return st.as_dict()

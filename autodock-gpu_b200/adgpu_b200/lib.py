@@ -33,6 +33,7 @@ SIGNATURES = {
     "adgpu_dock_resident": (_i, [_i, _u32, _u64, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
     "adgpu_dock_resident_autostop": (_i, [_i, _u32, _u64, _u32, _u32, C.c_float, _u64,
                                           _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "adgpu_dock_stats_get": (_i, [_vp]),
     "adgpu_grid_read": (_i, [C.c_char_p, _vp]),
     "adgpu_grid_from_values": (_i, [_vp, C.c_double, _vp, _i, _vp, _vp, _vp]),
     "adgpu_grid_free": (None, [_vp]),

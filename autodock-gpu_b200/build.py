@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib", "libadgpu_b200.so")
-SOURCES = ["adgpu_api.cu", "adgpu_tables.cu", "adgpu_engine.cu", "adgpu_compat.cu", "adgpu_prep.cpp", "adgpu_frontend.cpp", "adgpu_probe.cu", "adgpu_noalloc.cu"]
+SOURCES = ["adgpu_api.cu", "adgpu_tables.cu", "adgpu_engine.cu", "adgpu_compat.cu", "adgpu_prep.cpp", "adgpu_frontend.cpp", "adgpu_probe.cu", "adgpu_noalloc.cu", "adgpu_pipeline.cu"]
 # Flushed single-precision denormals: part of the -use_fast_math the
 # reference builds its CUDA kernels with (Makefile.Cuda:97-103); it takes 7%
 # off a scoring (B200, 45 atoms, 777 pairs).  Division, square root and

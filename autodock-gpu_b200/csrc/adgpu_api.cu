@@ -11,6 +11,7 @@
 #include "adgpu_kernels.cuh"
 #include "adgpu_autostop.cuh"
 #include "adgpu_tables.h"
+#include "adgpu_pipeline.h"
 
 #ifndef ADGPU_MIN_CTAS
 #define ADGPU_MIN_CTAS 6     // 6 CTAs x 4 warps per SM: <= 80 registers, no spills
@@ -237,6 +238,8 @@ struct ApiState {
 	LigandTables tables;       // host-repacked + device copy
 	int tpp = 0;               // threads per pose; 0: chosen per launch (auto_tpp)
 	unsigned int* counters = nullptr;   // library-owned work counters of the local-search launches
+	bool pipeline = true;      // adgpu_dock_resident without AutoStop runs the pipelined loop where it applies
+	PipeScratch pipe;          // its scratch, kept between calls
 	std::mutex mu;
 };
 
@@ -276,6 +279,13 @@ adgpu_status dock_resident(ApiState& s, int lsmet, uint32_t runs, uint64_t max_e
                            int* autostopped)
 {
 	const adgpu_dockpars& dp = s.data.dockpars;
+	memset(&s.pipe.stats, 0, sizeof(s.pipe.stats));
+	if (as_frequency == 0 && s.pipeline && pipeline_applies(dp, runs)) {
+		*autostopped = 0;
+		KArgs base = make_args(s);
+		return dock_pipelined(base, s.pipe, lsmet, s.tpp, runs, max_evals, max_gens, c1, e1, c2, e2,
+		                      final_is_second, generations);
+	}
 	const uint32_t T = 64;
 	cudaStream_t st;
 	ADGPU_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
@@ -386,6 +396,7 @@ adgpu_status dock_resident(ApiState& s, int lsmet, uint32_t runs, uint64_t max_e
 	ADGPU_TRY(cudaMemcpy(&g, d_gen, sizeof(g), cudaMemcpyDeviceToHost), "gen read");
 	*generations = g;
 	*final_is_second = (int)(g & 1u);
+	s.pipe.stats.generations = g;
 	*autostopped = 0;
 	if (as_args.state) {
 		AutoStopState h;
@@ -417,6 +428,8 @@ adgpu_status adgpu_set_kernels_gpu_data(const adgpu_gpudata* data)
 	if (st != ADGPU_OK) return st;
 	s.tpp = 0;
 	if (const char* t = getenv("ADGPU_THREADS_PER_POSE")) s.tpp = atoi(t);
+	s.pipeline = true;
+	if (const char* t = getenv("ADGPU_DOCK_PIPELINE")) s.pipeline = atoi(t) != 0;
 	if (!s.counters) ADGPU_CUDA(cudaMalloc(&s.counters, 16 * sizeof(unsigned int)), "work counters");
 	s.ready = true;
 	return ADGPU_OK;
@@ -517,6 +530,13 @@ adgpu_status adgpu_score_terms(uint32_t n, const float* genotypes, float* energi
 {
 	if (!genotypes || !energies || !terms) return fail(ADGPU_ERR_ARG, "null buffer");
 	return run_kind(8, n, 64, nullptr, nullptr, const_cast<float*>(genotypes), energies, terms);
+}
+
+adgpu_status adgpu_dock_stats_get(adgpu_dock_stats* out)
+{
+	if (!out) return fail(ADGPU_ERR_ARG, "null out");
+	*out = api().pipe.stats;
+	return ADGPU_OK;
 }
 
 adgpu_status adgpu_dock_resident(int lsmet, uint32_t num_runs, uint64_t max_evals, uint32_t max_gens,

@@ -156,6 +156,8 @@ struct Group {
 	int bar_id;        // named barrier for TPP > 32
 	float* red;        // TPP/32 * 8 floats of scratch for cross-warp reductions
 
+	__device__ static constexpr int size() { return TPP; }
+
 	// Barrier ids are immediates so that a kernel reserves only the ids it
 	// uses (a register id makes ptxas reserve all 16, which caps resident
 	// CTAs per SM at 4).  A 128-thread group is a whole 128-thread CTA.

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "adgpu_kernels.cuh"
+#include "adgpu_queue.cuh"
 #include "adgpu_prep.h"
 #include "adgpu_result.h"
 #include "adgpu_tables.h"
@@ -76,7 +77,7 @@ constexpr int kEngineThreads = 128;
 enum : uint32_t { kTaskStart = 0, kTaskInit = 1, kTaskGA = 2, kTaskLS = 3 };
 constexpr uint32_t kTaskIdxBits = 11;                          // entity / chunk index < 2048
 constexpr uint32_t kMaxTickRuns = 1u << (32 - kTaskIdxBits - 2); // run index bits
-constexpr int kSlotSpin = 1 << 20;                             // wait for a reserved slot's write
+constexpr int kSlotSpin = 1 << 20;                             // polls of a reserved slot's write
 constexpr long long kIdleNs = 20000000;                        // an idle worker retires after 20 ms
 
 __host__ __device__ constexpr uint32_t task_word(uint32_t w, uint32_t kind, uint32_t idx)
@@ -84,22 +85,8 @@ __host__ __device__ constexpr uint32_t task_word(uint32_t w, uint32_t kind, uint
 	return (w << (kTaskIdxBits + 2)) | (kind << kTaskIdxBits) | idx;
 }
 
-struct QueueCtl {
-	unsigned long long head;    // next position to pop
-	unsigned long long tail;    // next position to push
-	int alive;                  // runs of the class not yet retired in this tick
-	int err;                    // nonzero: a reserved slot was never written
-	int workers;                // pose groups that served this class
-	int pad;
-	// accounting (globaltimer ns): time pose groups spent on tasks, tasks done,
-	// first worker start and last worker exit
-	unsigned long long busy_ns, tasks, t_first, t_last;
-};
-
-struct TickClass {
-	unsigned long long* slots;  // ring: (lap << 32) | task word, lap = position / cap + 1
-	QueueCtl* ctl;
-	uint32_t cap;
+// A class's ring (adgpu_queue.cuh) and the CTAs that serve it.
+struct TickClass : TaskRing {
 	int cta_end;                // this class's CTAs are [previous class's cta_end, cta_end)
 	int group_bytes;            // shared memory per pose group
 };
@@ -126,64 +113,6 @@ struct GroupHdr {
 	int bi[4];
 };
 constexpr int kHdrBytes = (int)((sizeof(GroupHdr) + 15) / 16 * 16);
-
-__device__ __forceinline__ long long global_ns()
-{
-	long long t;
-	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-	return t;
-}
-
-// Next task of a class, or -1 when the worker should stop: every run of the
-// class has retired, the tick's time is up (tasks still queued stay for the
-// next tick), the queue stayed empty for kIdleNs, or (error) a reserved slot
-// was never written.
-__device__ int queue_pop(const TickClass& C, long long deadline)
-{
-	volatile QueueCtl* vq = C.ctl;
-	long long idle_since = -1;
-	for (int spins = 0; spins < (1 << 28); spins++) {
-		if (deadline && global_ns() > deadline) return -1;
-		const unsigned long long h = vq->head, t = vq->tail;
-		if (h < t) {
-			if (atomicCAS(&C.ctl->head, h, h + 1) != h) continue;
-			const unsigned long long want = h / C.cap + 1;
-			volatile unsigned long long* s = C.slots + (h % C.cap);
-			for (int k = 0; k < kSlotSpin; k++) {
-				const unsigned long long v = *s;
-				if ((v >> 32) == want) {
-					__threadfence();
-					return (int)(uint32_t)v;
-				}
-				__nanosleep(64);
-			}
-			atomicExch(&C.ctl->err, 1);
-			return -1;
-		}
-		if (vq->alive <= 0) return -1;
-		const long long now = global_ns();
-		if (idle_since < 0) idle_since = now;
-		else if (now - idle_since > kIdleNs) return -1;
-		__nanosleep(400);
-	}
-	atomicExch(&C.ctl->err, 2);
-	return -1;
-}
-
-// Pushes tasks task_word(w, kind, i), i in [0, n), with the whole group.
-template <int TPP>
-__device__ void queue_push(const TickClass& C, uint32_t w, uint32_t kind, int n, const Group<TPP>& G, GroupHdr& H)
-{
-	if (G.rank == 0) H.pos = atomicAdd(&C.ctl->tail, (unsigned long long)n);
-	G.sync();
-	const unsigned long long p0 = H.pos;
-	__threadfence();
-	for (int i = G.rank; i < n; i += TPP) {
-		const unsigned long long p = p0 + (unsigned long long)i;
-		atomicExch(C.slots + (p % C.cap), ((p / C.cap + 1) << 32) | task_word(w, kind, (uint32_t)i));
-	}
-	G.sync();
-}
 
 template <int TPP>
 __device__ int group_isum(int v, const Group<TPP>& G, GroupHdr& H)
@@ -253,7 +182,7 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 	for (;;) {
 		if (G.rank == 0) {
 			if (H.t_task) H.busy += (unsigned long long)(global_ns() - H.t_task);
-			H.task = queue_pop(C, H.deadline);
+			H.task = ring_pop(C, H.deadline);
 			H.t_task = H.task >= 0 ? global_ns() : 0;
 			H.ntask += H.task >= 0;
 		}
@@ -321,7 +250,7 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 		if (kind == kTaskGA && L > 0 && a.dp.lsearch_rate != 0.0f) {
 			if (G.rank == 0) { rq.pending[run] = L; __threadfence(); }
 			G.sync();
-			queue_push<TPP>(C, w, kTaskLS, L, G, H);
+			ring_push(C, task_word(w, kTaskLS, 0), L, G, H.pos);
 			continue;
 		}
 		if (kind == kTaskGA || kind == kTaskLS) {
@@ -357,7 +286,7 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 			const int nch = (P + t.ga_chunk - 1) / t.ga_chunk;
 			if (G.rank == 0) { rq.pending[run] = nch; __threadfence(); }
 			G.sync();
-			queue_push<TPP>(C, w, next == kNextGA ? kTaskGA : kTaskInit, nch, G, H);
+			ring_push(C, task_word(w, next == kNextGA ? kTaskGA : kTaskInit, 0), nch, G, H.pos);
 			continue;
 		}
 		if (next == kNextBest) best_of_run<TPP>(rq, run, H.cur, P, G, H);
@@ -830,6 +759,8 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 			t.cls[k].slots = E.d_slots + slot0[c];
 			t.cls[k].ctl = E.d_ctl + c;
 			t.cls[k].cap = (uint32_t)cap[c];
+			t.cls[k].slot_spin = kSlotSpin;
+			t.cls[k].idle_ns = kIdleNs;
 			any |= nr[k] > 0;
 		}
 		if (!any) continue;

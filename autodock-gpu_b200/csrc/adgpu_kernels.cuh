@@ -33,6 +33,19 @@ struct KArgs {
 	unsigned int* work_counter; // nullable: zeroed before the launch; pose groups take blocks from it
 };
 
+// The population buffers a block reads and writes: the launch's own
+// (bufs_of) or, in the pipelined docking loop, those of the block's
+// generation.  Passed apart from KArgs so that KArgs can stay a kernel
+// parameter read with constant offsets in the scorer.
+struct PopBufs {
+	const float* conf_cur;      // GA: current population
+	const float* e_cur;
+	float* conf;                // GA: next population; LS/initpop: population worked on
+	float* e;
+};
+
+__device__ __forceinline__ PopBufs bufs_of(const KArgs& a) { return PopBufs{a.conf_cur, a.e_cur, a.conf, a.e}; }
+
 // Per-group scratch carved from dynamic shared memory.
 struct GroupSmem {
 	PoseSmem pose;
@@ -126,13 +139,13 @@ __device__ __forceinline__ int ls_entity(const KArgs& a, uint32_t b, const Group
 // ADAM (cuda/kernel_adam.cu:55-396): bias-corrected, always max_num_of_iters.
 // ---------------------------------------------------------------------------
 template <int TPP, int METHOD>
-__device__ void gradient_ls_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+__device__ void gradient_ls_block(const KArgs& a, const PopBufs& pb, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
 {
 	const int P = a.dp.pop_size, NG = a.dp.num_of_genes;
 	const int run = (int)(b / a.dp.num_of_lsentities);
 	const int ent = ls_entity<TPP>(a, b, G, S);
 	const size_t idx = (size_t)run * P + ent;
-	const float* src = a.conf + idx * kGenotypeStride;
+	const float* src = pb.conf + idx * kGenotypeStride;
 	for (int k = G.rank; k < NG; k += TPP) {
 		S.gen[k] = src[k]; S.best[k] = S.gen[k]; S.grad[k] = 0.f; S.s1[k] = 0.f; S.s2[k] = 0.f;
 	}
@@ -176,7 +189,7 @@ __device__ void gradient_ls_block(const KArgs& a, uint32_t b, const Group<TPP>& 
 		}
 		G.sync();
 	} while (it < a.dp.max_num_of_iters && (METHOD == LS_ADAM || rho > 0.01f));
-	float* dst = a.conf + idx * kGenotypeStride;
+	float* dst = pb.conf + idx * kGenotypeStride;
 	for (int k = G.rank; k < NG; k += TPP) {
 		float v = S.best[k];
 		if (k >= 3) map_angle(v);
@@ -184,7 +197,7 @@ __device__ void gradient_ls_block(const KArgs& a, uint32_t b, const Group<TPP>& 
 	}
 	if (G.rank == 0) {
 		a.evals_new[idx] += (int)it;
-		a.e[idx] = best_e;
+		pb.e[idx] = best_e;
 	}
 	G.sync();
 }
@@ -194,19 +207,19 @@ __device__ void gradient_ls_block(const KArgs& a, uint32_t b, const Group<TPP>& 
 // alpha0 0.2, f_alpha 0.99, dt_max 10, dt0 = dt_max/3, stop at dt < 1e-6.
 // ---------------------------------------------------------------------------
 template <int TPP>
-__device__ void fire_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+__device__ void fire_block(const KArgs& a, const PopBufs& pb, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
 {
 	const float DT_INC = 1.2f, DT_DEC = 0.8f, ALPHA_START = 0.2f, ALPHA_DEC = 0.99f, DT_MAX = 10.0f, DT_MIN = 1e-6f;
 	const int P = a.dp.pop_size, NG = a.dp.num_of_genes;
 	const int run = (int)(b / a.dp.num_of_lsentities);
 	const int ent = ls_entity<TPP>(a, b, G, S);
 	const size_t idx = (size_t)run * P + ent;
-	const float* src = a.conf + idx * kGenotypeStride;
+	const float* src = pb.conf + idx * kGenotypeStride;
 	float* gen = S.gen; float* best = S.best; float* grad = S.grad;
 	float* cgen = S.s1; float* cgrad = S.s2; float* vel = S.s3;
 	for (int k = G.rank; k < NG; k += TPP) { gen[k] = src[k]; best[k] = gen[k]; }
 	G.sync();
-	float energy = a.e[idx];
+	float energy = pb.e[idx];
 	// initial gradient (the OpenCL kernel's gradient-only call, taken from the merged scorer)
 	score_pose<TPP, true>(a.L, gen, grad, S.pose, G);
 	auto sumsq = [&](const float* v) {
@@ -252,13 +265,13 @@ __device__ void fire_block(const KArgs& a, uint32_t b, const Group<TPP>& G, cons
 		}
 		G.sync();
 	} while (it < a.dp.max_num_of_iters && dt > DT_MIN);
-	float* dst = a.conf + idx * kGenotypeStride;
+	float* dst = pb.conf + idx * kGenotypeStride;
 	for (int k = G.rank; k < NG; k += TPP) {
 		float v = best[k];
 		if (k >= 3) map_angle(v);
 		dst[k] = v;
 	}
-	if (G.rank == 0) { a.evals_new[idx] += (int)it; a.e[idx] = best_e; }
+	if (G.rank == 0) { a.evals_new[idx] += (int)it; pb.e[idx] = best_e; }
 	G.sync();
 }
 
@@ -266,7 +279,7 @@ __device__ void fire_block(const KArgs& a, uint32_t b, const Group<TPP>& G, cons
 // Solis-Wets with SWAT3 step scaling (cuda/kernel3.cu:30-308).
 // ---------------------------------------------------------------------------
 template <int TPP>
-__device__ void sw_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+__device__ void sw_block(const KArgs& a, const PopBufs& pb, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
 {
 	const int P = a.dp.pop_size, NG = a.dp.num_of_genes;
 	const uint32_t T = a.ref_threads;
@@ -274,14 +287,14 @@ __device__ void sw_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const 
 	const int ent = ls_entity<TPP>(a, b, G, S);
 	const size_t idx = (size_t)run * P + ent;
 	float* gen = S.gen; float* cand = S.s1; float* dev = S.s2; float* bias = S.s3;
-	const float* src = a.conf + idx * kGenotypeStride;
+	const float* src = pb.conf + idx * kGenotypeStride;
 	for (int k = G.rank; k < NG; k += TPP) { gen[k] = src[k]; cand[k] = gen[k]; bias[k] = 0.f; dev[k] = 0.f; }
 	for (uint32_t r = G.rank; r < T; r += TPP) S.st[r] = a.prng[b * T + r];
 	G.sync();
 	const int gs = (a.dp.true_ligand_atoms == 0) * 6;
 	const float lig_scale = 1.0f / sqrtf((float)a.dp.num_of_atoms);
 	const float gene_scale = 1.0f / sqrtf((float)NG);
-	float cur_e = a.e[idx], rho = 1.0f;
+	float cur_e = pb.e[idx], rho = 1.0f;
 	int succ = 0, fail = 0, iters = 0, evals = 0;
 	while (iters < (int)a.dp.max_num_of_iters && rho > a.dp.rho_lower_bound) {
 		// reference lane r owns genes gs + r, gs + r + T, ... (its own LCG stream)
@@ -324,14 +337,14 @@ __device__ void sw_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const 
 		else if (fail >= (int)a.dp.cons_limit) { rho *= 0.5f; fail = 0; }
 		G.sync();
 	}
-	float* dst = a.conf + idx * kGenotypeStride;
+	float* dst = pb.conf + idx * kGenotypeStride;
 	for (int k = gs + G.rank; k < NG; k += TPP) {
 		float v = gen[k];
 		if (k >= 3) map_angle(v);
 		dst[k] = v;
 	}
 	for (uint32_t r = G.rank; r < T; r += TPP) a.prng[b * T + r] = S.st[r];
-	if (G.rank == 0) { a.evals_new[idx] += evals; a.e[idx] = cur_e; }
+	if (G.rank == 0) { a.evals_new[idx] += evals; pb.e[idx] = cur_e; }
 	G.sync();
 }
 
@@ -355,7 +368,7 @@ __device__ __forceinline__ void warp_minimum2(int lane, float& v, int& k)
 }
 
 template <int TPP>
-__device__ void ga_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+__device__ void ga_block(const KArgs& a, const PopBufs& pb, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
 {
 	const int P = a.dp.pop_size, NG = a.dp.num_of_genes;
 	const uint32_t T = a.ref_threads;
@@ -369,11 +382,11 @@ __device__ void ga_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const 
 			for (int w = 0; w < nw; w++) {
 				const int t = w * 32 + lane;
 				float v; int k;
-				if (t < P && t < (int)T) { k = (int)b + t; v = a.e_cur[b + t]; }
+				if (t < P && t < (int)T) { k = (int)b + t; v = pb.e_cur[b + t]; }
 				else { k = -1; v = FLT_MAX; }
 				if (t < (int)T)
 					for (int i = (int)b + (int)T + t; i < (int)b + P; i += (int)T) {
-						float e = a.e_cur[i];
+						float e = pb.e_cur[i];
 						if (e < v) { k = i; v = e; }
 					}
 				warp_minimum2(lane, v, k);
@@ -383,11 +396,11 @@ __device__ void ga_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const 
 			}
 			if (lane >= (int)(T / 32)) { wv = FLT_MAX; wk = -1; }
 			warp_minimum2(lane, wv, wk);
-			if (lane == 0) { S.misc[0] = wk; a.e[b] = wv; a.evals_new[b] = 0; }
+			if (lane == 0) { S.misc[0] = wk; pb.e[b] = wv; a.evals_new[b] = 0; }
 		}
 		G.sync();
 		const int src = S.misc[0];
-		for (int k = G.rank; k < NG; k += TPP) a.conf[(size_t)b * kGenotypeStride + k] = a.conf_cur[(size_t)src * kGenotypeStride + k];
+		for (int k = G.rank; k < NG; k += TPP) pb.conf[(size_t)b * kGenotypeStride + k] = pb.conf_cur[(size_t)src * kGenotypeStride + k];
 		G.sync();
 		return;
 	}
@@ -403,15 +416,15 @@ __device__ void ga_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const 
 	int cand[4]; float ce[4];
 	for (int i = 0; i < 4; i++) {
 		cand[i] = (int)((float)P * rn[i]);
-		ce[i] = a.e_cur[run * P + cand[i]];
+		ce[i] = pb.e_cur[run * P + cand[i]];
 	}
 	int par[2];
 	for (int i = 0; i < 2; i++) {
 		if (ce[2 * i] < ce[2 * i + 1]) par[i] = (rn[4 + i] < a.dp.tournament_rate) ? cand[2 * i] : cand[2 * i + 1];
 		else par[i] = (rn[4 + i] < a.dp.tournament_rate) ? cand[2 * i + 1] : cand[2 * i];
 	}
-	const float* p0 = a.conf_cur + (size_t)(run * P + par[0]) * kGenotypeStride;
-	const float* p1 = a.conf_cur + (size_t)(run * P + par[1]) * kGenotypeStride;
+	const float* p0 = pb.conf_cur + (size_t)(run * P + par[0]) * kGenotypeStride;
+	const float* p1 = pb.conf_cur + (size_t)(run * P + par[1]) * kGenotypeStride;
 	if (rn[6] < a.dp.crossover_rate) {
 		int c0 = (int)((float)(NG - 1) * rn[7]), c1 = (int)((float)(NG - 1) * rn[8]);
 		if (c1 < c0) { int t = c1; c1 = c0; c0 = t; }
@@ -437,10 +450,24 @@ __device__ void ga_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const 
 	}
 	G.sync();
 	const float e = score_pose<TPP, false>(a.L, off, nullptr, S.pose, G);
-	if (G.rank == 0) { a.e[b] = e; a.evals_new[b] = 1; }
-	for (int g = G.rank; g < NG; g += TPP) a.conf[(size_t)b * kGenotypeStride + g] = off[g];
+	if (G.rank == 0) { pb.e[b] = e; a.evals_new[b] = 1; }
+	for (int g = G.rank; g < NG; g += TPP) pb.conf[(size_t)b * kGenotypeStride + g] = off[g];
 	G.sync();
 }
+
+// The blocks above on the launch's own population buffers.
+template <int TPP, int METHOD>
+__device__ __forceinline__ void gradient_ls_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+{ gradient_ls_block<TPP, METHOD>(a, bufs_of(a), b, G, S); }
+template <int TPP>
+__device__ __forceinline__ void fire_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+{ fire_block<TPP>(a, bufs_of(a), b, G, S); }
+template <int TPP>
+__device__ __forceinline__ void sw_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+{ sw_block<TPP>(a, bufs_of(a), b, G, S); }
+template <int TPP>
+__device__ __forceinline__ void ga_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+{ ga_block<TPP>(a, bufs_of(a), b, G, S); }
 
 // Initial population energies (cuda/kernel1.cu:26-55).
 template <int TPP>

@@ -264,8 +264,18 @@ adgpu_status adgpu_score_genotypes_noalloc(const adgpu_gpudata* data, uint32_t n
  * already resident in conformations1/energies1 (initpop and sum_evals must
  * have run, as in the reference).  On return the final
  * population is in the buffers reported through *final_is_second (0: 1, 1: 2)
- * and *generations holds the number of generations executed.  Graph-captures
- * the per-generation launch sequence. */
+ * and *generations holds the number of generations executed.
+ * With a 100 % local-search rate (num_of_lsentities == pop_size, the
+ * reference's default) the loop is one persistent launch in which every run
+ * starts its next generation as soon as its own local searches end, up to
+ * three generations ahead of the stop test; generations run past the stop are
+ * discarded, so populations, energies, evaluation counts and the generation
+ * count are those of the generation-synchronous loop (only the PRNG states
+ * and the per-entity evaluation counters keep the discarded generations'
+ * draws).  Otherwise, or with ADGPU_DOCK_PIPELINE=0 in the environment of
+ * adgpu_set_kernels_gpu_data, it graph-captures the per-generation launch
+ * sequence.  Uses the legacy default stream; returns when the loop has
+ * ended. */
 adgpu_status adgpu_dock_resident(int lsmet, uint32_t num_runs, uint64_t max_evals, uint32_t max_gens,
                                  float* conformations1, float* energies1,
                                  float* conformations2, float* energies2,
@@ -286,6 +296,22 @@ adgpu_status adgpu_dock_resident_autostop(int lsmet, uint32_t num_runs, uint64_t
                                           float* conformations1, float* energies1,
                                           float* conformations2, float* energies2,
                                           int* final_is_second, uint32_t* generations, int* autostopped);
+
+/* Accounting of the last adgpu_dock_resident call on this process (no
+ * counterpart in the reference). */
+typedef struct {
+	int      pipelined;               /* 1: the pipelined loop ran; 0: the per-generation launches */
+	int      threads_per_pose;        /* pipelined loop: threads per pose group */
+	int      pose_groups;             /* pipelined loop: pose groups of the launch */
+	uint32_t generations;             /* generations run (as reported by the call) */
+	uint32_t generations_discarded;   /* most generations any run ran past the stop */
+	uint64_t tasks;                   /* GA chunks and local searches executed */
+	uint64_t parks;                   /* times a run waited for a stop test before its next generation */
+	double   busy_s;                  /* summed time pose groups spent on tasks */
+	double   span_s;                  /* first pose group start to last pose group exit */
+} adgpu_dock_stats;
+
+adgpu_status adgpu_dock_stats_get(adgpu_dock_stats* out);
 
 /* ---------------------------------------------------------------------------
  * Front end: the input side of the path.  Reads AutoDock-4 grid maps and
