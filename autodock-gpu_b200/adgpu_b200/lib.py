@@ -47,7 +47,6 @@ SIGNATURES = {
     "adgpu_ligand_free": (None, [_vp]),
     "adgpu_ligand_tables": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "adgpu_ligand_population": (_i, [_vp, _vp, C.c_size_t, _vp, C.c_size_t]),
-    "adgpu_measure_fp32_peak": (_i, [_vp, C.c_size_t, _vp]),
     "adgpu_last_error": (C.c_char_p, []),
     "adgpu_version": (C.c_char_p, []),
 }

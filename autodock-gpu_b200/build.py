@@ -13,7 +13,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib", "libadgpu_b200.so")
-SOURCES = ["adgpu_api.cu", "adgpu_tables.cu", "adgpu_engine.cu", "adgpu_compat.cu", "adgpu_prep.cpp", "adgpu_frontend.cpp", "adgpu_probe.cu", "adgpu_noalloc.cu", "adgpu_pipeline.cu"]
+# bench-only: the FP32 FMA peak probe (csrc/probe), not part of the product library
+PROBE_OUT = os.path.join(HERE, "lib", "libadgpu_probe.so")
+PROBE_SRC = os.path.join(CSRC, "probe", "fp32_peak.cu")
+SOURCES = ["adgpu_api.cu", "adgpu_tables.cu", "adgpu_engine.cu", "adgpu_compat.cu", "adgpu_prep.cpp", "adgpu_frontend.cpp", "adgpu_noalloc.cu", "adgpu_pipeline.cu"]
 # Flushed single-precision denormals: part of the -use_fast_math the
 # reference builds its CUDA kernels with (Makefile.Cuda:97-103); it takes 7%
 # off a scoring (B200, 45 atoms, 777 pairs).  Division, square root and
@@ -74,6 +77,15 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     return OUT
 
 
+def build_probe(force: bool = False, verbose: bool = False) -> str:
+    if not force and os.path.exists(PROBE_OUT) and os.path.getmtime(PROBE_OUT) > os.path.getmtime(PROBE_SRC):
+        return PROBE_OUT
+    os.makedirs(os.path.dirname(PROBE_OUT), exist_ok=True)
+    flags = [f for f in NVCC_FLAGS if f != "-ftz=true"]
+    _run([nvcc()] + flags + ["-o", PROBE_OUT, PROBE_SRC, "-lcudart"], verbose)
+    return PROBE_OUT
+
+
 def build_oracle() -> None:
     r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "-j8"], capture_output=True, text=True)
     if r.returncode != 0:
@@ -84,6 +96,7 @@ def build_oracle() -> None:
 
 if __name__ == "__main__":
     build_lib(force="--force" in sys.argv, verbose=True)
+    build_probe(force="--force" in sys.argv, verbose=True)
     if "--no-oracle" not in sys.argv:
         build_oracle()
     print(OUT)

@@ -17,7 +17,8 @@ ligands are independent, there is no data-path collective (replicas), and
 
 --impl reference times the reference's algorithm on the host cores: the C
 restatement of the reference kernels (oracle/, one pose per thread, all
-host threads) on a bounded sample of the same workload.
+host threads), on inputs prepared by the reference's own front end
+(oracle/_ref), one complete generation of the same docking per step.
 """
 from __future__ import annotations
 
@@ -179,61 +180,129 @@ class ClockSampler:
                 "samples": len(sm), "source": "nvidia-smi"}
 
 
-def cpu_baseline(lig, lsmet: str, budget_s: float = 15.0):
-    """The oracle (C restatement of the reference kernels, one pose per host
-    thread) on a bounded sample: local searches of the initial population."""
-    from oracle import oraclepy
-    from adgpu_b200 import abi
+# ---------------------------------------------------------------------------
+# CPU side: the oracle (C restatement of the reference kernels, one pose per
+# host thread) on inputs prepared by the reference's own front end
+# (oracle/_ref), so that neither this repository's library nor its front end
+# is on that path.
+# ---------------------------------------------------------------------------
+def _reference_inputs(config_id: int, npts: int, n_heavy: int, n_tors: int, nrun: int, lsmet: str):
+    """Writes the seeded synthetic maps and ligand as .fld/.map/.pdbqt files and
+    prepares them with the reference's own front end (oracle/_ref)."""
+    import tempfile
+    from adgpu_b200 import synth          # numpy only: no library is loaded
+    from oracle import oraclepy, refpy
+    w = WORKLOAD
+    d = tempfile.mkdtemp(prefix=f"adgpu_ref{config_id}_")
+    spec = synth.grid_spec(npts, w["types"], seed=12345 + config_id)
+    fld = synth.write_maps(spec, synth.make_maps(spec), d)
+    lig_path = os.path.join(d, "ligand.pdbqt")
+    synth.write_ligand(synth.ligand_for(config_id, 0, n_heavy, n_tors), lig_path)
+    job = refpy.RefJob(["--ffile", fld, "--lfile", lig_path, "--nrun", str(nrun), "--seed",
+                        ",".join(str(s) for s in w["seed"]), "--lsmet", lsmet, "--heuristics", "0", "--autostop", "0",
+                        "--nev", str(w["nev"]), "--psize", str(w["pop"])])
+    ht = oraclepy.tables_from_refjob(job)
+    return job, ht
+
+
+class OracleDocking:
+    """docking_with_gpu's generation loop (host/src/performdocking.cpp.Cuda:
+    684-831) over the oracle's kernels on the host cores."""
+
+    LS = {"ad": "gradient_minad", "sw": "perform_ls", "adam": "gradient_minadam", "fire": "gradient_minfire"}
+
+    def __init__(self, job, ht, lsmet: str, nthreads: int):
+        from adgpu_b200 import abi
+        self.ht, self.lsmet, self.nt = ht, lsmet, nthreads
+        dp = ht.dockpars
+        self.R, self.P, self.L = job.info.num_of_runs, dp.pop_size, dp.num_of_lsentities
+        n = self.R * self.P
+        self.prng = job.blob("prng").copy()
+        self.en = np.zeros(n, np.int32)
+        self.er = np.zeros(self.R, np.int32)
+        ht.bind_state(self.prng, self.en, self.er)
+        self.cur = job.blob("initpop").reshape(-1, abi.GENOTYPE_STRIDE)[:n].copy()
+        self.ecur = np.zeros(n, np.float32)
+        self.nxt, self.enxt = np.zeros_like(self.cur), np.zeros_like(self.ecur)
+        ht.call("calc_initpop", n, self.cur, self.ecur, nthreads)
+        ht.call("sum_evals", self.R)
+        self.generations = 0
+
+    def evals(self) -> int:
+        return int(self.er.sum())
+
+    def generation(self):
+        T = 64
+        self.ht.call("gen_and_eval_newpops", self.R * self.P, T, self.cur, self.ecur, self.nxt, self.enxt, self.nt)
+        self.ht.call(self.LS[self.lsmet], self.R * self.L, T, self.nxt, self.enxt, self.nt)
+        self.ht.call("sum_evals", self.R)
+        self.cur, self.nxt, self.ecur, self.enxt = self.nxt, self.cur, self.enxt, self.ecur
+        self.generations += 1
+
+    def run(self, nev: int, ngen: int = 42000):
+        """Until the mean evaluations per run reach nev (check_progress, :908-942)."""
+        while max(self.evals() / self.R / nev, self.generations / ngen) < 1.0:
+            self.generation()
+
+
+def cpu_baseline(lsmet: str, budget_s: float = 12.0):
+    """The workload's docking on the host cores (the oracle): complete
+    generations of the plain docking from its initial population for about
+    budget_s, plus one complete docking of the small CPU-runnable
+    configuration (40^3 maps, 16 heavy atoms / 4 torsions, nrun 10, 2.5M
+    evaluations per run)."""
+    w = WORKLOAD
     nthreads = os.cpu_count() or 1
-    ht = oraclepy.HostTables(lig.tables, lig.dockpars, _reference_grid_cache["grid"])
-    P = lig.dockpars.pop_size
-    runs = 2
-    pop = lig.initpop[:runs * P].copy()
-    en = np.zeros(runs * P, np.int32)
-    er = np.zeros(runs, np.int32)
-    ht.bind_state(lig.prng.copy(), en, er)
-    e = ht.score(pop, False, nthreads=nthreads)
-    fn = {"ad": "gradient_minad", "sw": "perform_ls", "adam": "gradient_minadam", "fire": "gradient_minfire"}[lsmet]
-    L = lig.dockpars.num_of_lsentities
-    evals, t0 = 0, time.perf_counter()
-    reps = 0
-    while time.perf_counter() - t0 < budget_s:
-        c = pop.copy()
-        ee = e.copy()
-        en[:] = 0
-        ht.call(fn, runs * L, 64, c, ee, nthreads)
-        evals += int(en.sum())
-        reps += 1
+    job, ht = _reference_inputs(w["config_id"], w["npts"], w["n_heavy"], w["n_tors"], w["nrun"], lsmet)
+    od = OracleDocking(job, ht, lsmet, nthreads)
+    e0, t0 = od.evals(), time.perf_counter()
+    while time.perf_counter() - t0 < budget_s or od.generations < 1:
+        od.generation()
     dt = time.perf_counter() - t0
-    return {"value": evals / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
-            "sample": f"{reps} x {lsmet} local search of {runs}x{L} entities of the workload's initial population "
-                      f"({evals} evals, {dt:.1f} s) on {nthreads} host threads"}
-
-
-_reference_grid_cache = {}
+    v = (od.evals() - e0) / dt
+    job1, ht1 = _reference_inputs(1, 40, 16, 4, 10, lsmet)
+    d1 = OracleDocking(job1, ht1, lsmet, nthreads)
+    t1 = time.perf_counter()
+    d1.run(w["nev"])
+    s1 = time.perf_counter() - t1
+    return {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{od.generations} complete generations (GA + {lsmet} local search + eval sums, 100 runs x 150) "
+                      f"of the workload's docking from its initial population ({od.evals() - e0} evals, {dt:.1f} s), "
+                      f"inputs prepared by the reference's own front end, on {nthreads} host threads",
+            "cfg1_full_docking": {"workload": "40^3 maps, 16 heavy atoms / 4 torsions, nrun 10, pop 150, nev 2.5M, "
+                                              f"lsmet {lsmet}", "seconds": s1, "generations": d1.generations,
+                                  "evals_per_s": d1.evals() / s1, "ligands_per_hour": 3600.0 / s1}}
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference algorithm on the host cores."""
+    """--impl reference: the reference's algorithm (the oracle, a C
+    restatement of its kernels; inputs from its own front end) on the host
+    cores.  A step is one complete generation of the workload's docking (GA,
+    local search and eval sums over all 100 runs), continuing from the
+    previous step; value = evaluations / second over the timed steps."""
     if rank != 0:
         return None
-    grid, lig = build_inputs(args.lsmet)
-    _reference_grid_cache["grid"] = grid.reference_layout()
-    steps = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(lig, args.lsmet, budget_s=max(3.0, 20.0 / max(1, args.steps + args.warmup)))
-        if i >= args.warmup:
-            steps.append(cb)
-    v = sum(s["value"] for s in steps) / len(steps)
     w = WORKLOAD
+    nthreads = os.cpu_count() or 1
+    job, ht = _reference_inputs(w["config_id"], w["npts"], w["n_heavy"], w["n_tors"], w["nrun"], args.lsmet)
+    od = OracleDocking(job, ht, args.lsmet, nthreads)
+    for _ in range(args.warmup):
+        od.generation()
+    e0, t0 = od.evals(), time.perf_counter()
+    for _ in range(args.steps):
+        od.generation()
+    dt = time.perf_counter() - t0
+    v = (od.evals() - e0) / dt
     evals_per_docking = w["nrun"] * w["nev"]
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * evals_per_docking / v,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+    sample = (f"generations {args.warmup + 1}-{args.warmup + args.steps} of the workload's docking ({od.evals() - e0} "
+              f"evals, {dt:.1f} s), one generation per step, on {nthreads} host threads")
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(1, args.steps),
+            "step": "one complete generation (GA + local search + eval sums, 100 runs x 150 entities)",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": _config(args), "ligands_per_hour": 3600.0 * v / evals_per_docking,
-            "cpu_baseline": steps[-1] | {"value": v},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    return line
 
 
 def _config(args):
@@ -260,67 +329,91 @@ def rank_aggregate(seconds: float, work: float, device, world: int):
     return float(t.item()), float(w.item())
 
 
+def fp32_peak(dev) -> float:
+    """Measured FP32 FMA throughput of the device (TFLOP/s), from the
+    bench-only probe library (autodock-gpu_b200/csrc/probe)."""
+    import ctypes as C
+    import torch
+    path = os.path.join(ROOT, "autodock-gpu_b200", "lib", "libadgpu_probe.so")
+    L = C.CDLL(path)
+    L.adgpu_probe_fp32_peak.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
+    scratch = torch.empty(4096 * 1024, dtype=torch.float32, device=dev)
+    peak = C.c_float(0)
+    rc = L.adgpu_probe_fp32_peak(C.c_void_p(scratch.data_ptr()), scratch.numel(), C.byref(peak))
+    if rc != 0:
+        raise RuntimeError(f"fp32 probe failed ({rc})")
+    return float(peak.value)
+
+
+def _roofline_inputs():
+    """DRAM traffic and issue figures per evaluation of the dominant kernel from
+    the last ncu capture (profiles/roofline_inputs.json: kernel, case, date)."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "roofline_inputs.json")))
+    except Exception:
+        return {}
+
+
 def run_engine(args, rank, world, local_rank):
+    import ctypes as C
     import torch
     from adgpu_b200 import device, dock, lib
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    grid, lig = build_inputs(args.lsmet, rank)
-    ref_grid = grid.reference_layout()
-    _reference_grid_cache["grid"] = ref_grid
     w = WORKLOAD
-    job = device.DeviceJob(lig.tables, lig.dockpars, ref_grid, w["nrun"], lig.prng, device=dev)
-    job.activate()
-    bufs = (*job.population(), *job.population())
-    init_dev = torch.from_numpy(lig.initpop).to(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    prng0 = job.prng.clone()
+    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def one_docking():
-        job.prng.copy_(prng0)
-        return dock.dock(job, init_dev, args.lsmet, w["nev"], 42000, buffers=bufs)
+    def setup(lsmet):
+        grid, lig = build_inputs(lsmet, rank)
+        ref_grid = grid.reference_layout()
+        job = device.DeviceJob(lig.tables, lig.dockpars, ref_grid, w["nrun"], lig.prng, device=dev)
+        job.activate()
+        bufs = (*job.population(), *job.population())
+        init_dev = torch.from_numpy(lig.initpop).to(dev)
+        return grid, lig, ref_grid, job, bufs, init_dev, job.prng.clone()
 
-    for _ in range(args.warmup):
-        one_docking()
+    def timed_dockings(job, bufs, init_dev, prng0, lsmet, steps):
+        times, evals, gens, res = [], 0, 0, None
+        for _ in range(steps):
+            job.prng.copy_(prng0)
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev_a.record()
+            res = dock.dock(job, init_dev, lsmet, w["nev"], 42000, buffers=bufs)
+            ev_b.record()
+            torch.cuda.synchronize()
+            times.append(ev_a.elapsed_time(ev_b) / 1e3)
+            evals += int(res.evals_per_run.sum())
+            gens += res.generations
+        return times, evals, gens, res
+
+    grid, lig, ref_grid, job, bufs, init_dev, prng0 = setup(args.lsmet)
+    timed_dockings(job, bufs, init_dev, prng0, args.lsmet, args.warmup)
     torch.cuda.synchronize()
     sampler = ClockSampler(local_rank)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     sampler.start()
-    times, evals, gens = [], 0, 0
-    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        ev_a.record()
-        res = one_docking()
-        ev_b.record()
-        torch.cuda.synchronize()
-        times.append(ev_a.elapsed_time(ev_b) / 1e3)
-        evals += int(res.evals_per_run.sum())
-        gens += res.generations
+    times, evals, gens, res = timed_dockings(job, bufs, init_dev, prng0, args.lsmet, args.steps)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    t_local = sum(times)
-    t_all, ev_all = rank_aggregate(t_local, evals, dev, world)
+    loop_stats = dock.last_stats()
+    t_all, ev_all = rank_aggregate(sum(times), evals, dev, world)
     ev_all = int(ev_all)
     value = ev_all / t_all
     best = float(res.energies.min().item())
 
     # --- end to end through the public API with host buffers -------------------
-    host_grid = ref_grid
-    host_tables = lig.tables
-    host_pop = np.ascontiguousarray(lig.initpop, np.float32)
-    host_prng = lig.prng
-    e2e_times, e2e_evals = [], 0
-    h2d = host_grid.nbytes + sum(np.asarray(t).nbytes for t in host_tables.values()) + host_pop.nbytes + host_prng.nbytes
-    d2h = 0
-    for i in range(max(1, min(args.steps, 2))):
+    host_tables, host_pop, host_prng = lig.tables, np.ascontiguousarray(lig.initpop, np.float32), lig.prng
+    h2d = ref_grid.nbytes + sum(np.asarray(t).nbytes for t in host_tables.values()) + host_pop.nbytes + host_prng.nbytes
+    e2e_times, e2e_evals, d2h = [], 0, 0
+    for i in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        j2 = device.DeviceJob(host_tables, lig.dockpars, host_grid, w["nrun"], host_prng, device=dev)
+        j2 = device.DeviceJob(host_tables, lig.dockpars, ref_grid, w["nrun"], host_prng, device=dev)
         j2.activate()
         pop_dev = torch.from_numpy(host_pop).to(dev)
         r2 = dock.dock(j2, pop_dev, args.lsmet, w["nev"], 42000)
@@ -334,55 +427,51 @@ def run_engine(args, rank, world, local_rank):
     e2e_t, e2e_all = rank_aggregate(sum(e2e_times), e2e_evals, dev, world)
     e2e_value = e2e_all / e2e_t
 
-    # --- roofline of the dominant kernel (the local search) -------------------------
+    # --- roofline of the dominant kernel: the docking loop's persistent launch ---
     cm = cost_model(lig)
     roof = None
     if rank == 0:
-        mid = dock.dock(job, init_dev, args.lsmet, w["nev"], 10, buffers=bufs)   # a mid-docking population
-        c_mid, e_mid = mid.conformations.clone(), mid.energies.clone()
-        entry = {"ad": "adgpu_gradient_minad", "sw": "adgpu_perform_ls", "adam": "adgpu_gradient_minadam",
-                 "fire": "adgpu_gradient_minfire"}[args.lsmet]
-        L = lig.dockpars.num_of_lsentities
-        durs, ls_evals = [], []
-        for _ in range(3):
-            c, e = c_mid.clone(), e_mid.clone()
-            job.evals_new.zero_()
+        R, P = w["nrun"], w["pop"]
+        c1, e1, c2, e2 = bufs
+        durs, loop_evals, ga_evals = [], [], []
+        for _ in range(2):
+            job.prng.copy_(prng0)
+            c1.copy_(init_dev[:R * P])
+            job.evals_runs.zero_()
+            lib.call("adgpu_calc_initpop", R * P, 64, c1, e1)
+            lib.call("adgpu_sum_evals", R, 64)
             flush.zero_()
             torch.cuda.synchronize()
+            fin, gn = C.c_int(0), C.c_uint32(0)
             ev_a.record()
-            lib.call(entry, w["nrun"] * L, 64, c, e)
+            lib.call("adgpu_dock_resident", dock.LSMET[args.lsmet], R, w["nev"], 42000, c1, e1, c2, e2,
+                     C.byref(fin), C.byref(gn))
             ev_b.record()
             torch.cuda.synchronize()
             durs.append(ev_a.elapsed_time(ev_b) / 1e3)
-            ls_evals.append(int(job.evals_new.sum().item()))
+            loop_evals.append(int(job.evals_runs.sum().item()) - R * P)
+            ga_evals.append(gn.value * R * (P - 1))         # one per new entity, none for the elite
         dur = statistics.mean(durs)
-        flop_per_eval = cm["flop_grad"] if args.lsmet != "sw" else cm["flop_energy"]
-        achieved = statistics.mean(ls_evals) * flop_per_eval / dur / 1e12
-        scratch = torch.empty(4096 * 1024, dtype=torch.float32, device=dev)
-        import ctypes as C
-        peak = C.c_float(0)
-        lib.call("adgpu_measure_fp32_peak", scratch, scratch.numel(), C.byref(peak))
-        traffic = issue = instr = None
-        tfile = os.path.join(ROOT, "profiles", "ls_kernel_traffic.json")
-        if os.path.exists(tfile):
-            try:
-                prof = json.load(open(tfile))
-                traffic = prof.get(args.lsmet)
-                issue = prof.get(f"{args.lsmet}_issue_active")
-                instr = prof.get(f"{args.lsmet}_warp_instructions_per_eval")
-            except Exception:
-                traffic = None
-        roof = {"bound": "fp32", "achieved": achieved, "peak": float(peak.value), "unit": "TFLOP/s",
-                "frac": achieved / float(peak.value), "traffic": traffic,
-                "traffic_source": "ncu dram bytes per launch of this launch shape (profiles/ls_kernel_traffic.json)",
-                "peak_source": "measured in this run (FMA-chain probe, adgpu_measure_fp32_peak); "
+        n_loop, n_ga = statistics.mean(loop_evals), statistics.mean(ga_evals)
+        flop_ls = cm["flop_grad"] if args.lsmet != "sw" else cm["flop_energy"]
+        flop = (n_loop - n_ga) * flop_ls + n_ga * cm["flop_energy"]
+        achieved = flop / dur / 1e12
+        peak = fp32_peak(dev)
+        ri = _roofline_inputs().get(args.lsmet, {})
+        traffic = ri.get("dram_bytes_per_eval")
+        roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic * n_loop if traffic else None,
+                "traffic_source": (f"ncu dram__bytes_read+write per evaluation of {ri.get('kernel')} on "
+                                   f"{ri.get('case')} (capture of {ri.get('date')}, profiles/roofline_inputs.json) "
+                                   "x this launch's evaluations") if traffic else "no capture of this kernel",
+                "peak_source": "measured in this run (FMA-chain probe, bench-only libadgpu_probe.so); "
                                "MEASURED_PEAKS.json has no FP32 figure",
-                # the kernel is bound by instruction issue, not by a pipe: the
-                # share of issue slots it uses (ncu, same launch shape)
-                "issue_slots_active": issue, "warp_instructions_per_eval": instr,
-                "kernel": entry, "launch_ms": dur * 1e3, "evals_per_launch": statistics.mean(ls_evals),
-                "flop_per_eval": flop_per_eval, "bytes_per_eval": cm["bytes"],
-                "hbm_frac_of_measured": (statistics.mean(ls_evals) * cm["bytes"] / dur / 1e9) / _hbm_peak()}
+                "issue_slots_active": ri.get("issue_active"), "warp_instructions_per_eval": ri.get("warp_instr_per_eval"),
+                "kernel": "pipe_kernel (adgpu_dock_resident: the whole generation loop, one persistent launch)",
+                "launch_ms": dur * 1e3, "evals_per_launch": n_loop, "ga_evals_per_launch": n_ga,
+                "flop_per_eval": {"local_search": flop_ls, "ga": cm["flop_energy"]}, "bytes_per_eval": cm["bytes"],
+                "hbm_frac_of_measured": (n_loop * cm["bytes"] / dur / 1e9) / _hbm_peak(),
+                "pose_group_utilisation": dock.last_stats().get("utilisation")}
 
     line = None
     if rank == 0:
@@ -391,16 +480,26 @@ def run_engine(args, rank, world, local_rank):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-                "config": _config(args) | {"n_gpus": world},
+                "config": _config(args),
                 "ligands_per_hour": 3600.0 * world * args.steps / t_all,
                 "generations_per_docking": gl, "best_energy": best,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-                # per docking: initpop + sum_evals + batches of 4 graphs of 2 generations x 4 kernels, until
-                # the batch that sees the stop, plus the 6 batches queued behind it (their kernels return at entry)
-                "gpu_launches": int(args.steps * (2 + 32 * (-(-(gl + 1) // 8) + 6))),
+                # per docking: initpop, eval sums, then the loop's init, persistent and final kernels
+                "gpu_launches": int(args.steps * 5),
+                "docking_loop": loop_stats,
                 "clocks": clocks, "roofline": roof, "cost_model": cm}
+        # the same docking with the other local search of the plain configuration (sw <-> ad)
+        other = "sw" if args.lsmet != "sw" else "ad"
+        _, _, _, job_o, bufs_o, init_o, prng_o = setup(other)
+        timed_dockings(job_o, bufs_o, init_o, prng_o, other, 1)
+        t_o, ev_o, g_o, _ = timed_dockings(job_o, bufs_o, init_o, prng_o, other, max(2, min(args.steps, 5)))
+        line[f"lsmet_{other}"] = {"value": ev_o / sum(t_o), "unit": UNIT, "ms_per_step": 1e3 * sum(t_o) / len(t_o),
+                                  "steps": len(t_o), "generations_per_docking": g_o // len(t_o),
+                                  "ligands_per_hour": 3600.0 * len(t_o) / sum(t_o), "docking_loop": dock.last_stats()}
+        del job_o, bufs_o
+        job.activate()
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(lig, args.lsmet)
+            line["cpu_baseline"] = cpu_baseline(args.lsmet)
         # the single-GPU samples below run at N = 1 only (under torchrun the
         # other ranks would wait for them at the closing barrier)
         if world > 1:
@@ -457,6 +556,30 @@ def run_kernel_only(args):
     torch.cuda.synchronize()
     print(json.dumps({"mode": "ls-kernel", "kernel": entry, "nrun": nrun, "launches": args.steps,
                       "evals_last_launch": int(job.evals_new.sum().item())}))
+
+
+def run_loop_kernel(args):
+    """--mode loop-kernel: `--steps` pipelined dockings of the workload's ligand
+    with --nrun runs of --nev evaluations (the small case the ncu captures of
+    the docking loop's persistent kernel use); prints the loop's accounting."""
+    import torch
+    from adgpu_b200 import device, dock
+    grid, lig = build_inputs(args.lsmet)
+    ref_grid = grid.reference_layout()
+    w = WORKLOAD
+    nrun = args.nrun or w["nrun"]
+    job = device.DeviceJob(lig.tables, lig.dockpars, ref_grid, nrun, lig.prng)
+    job.activate()
+    init_dev = torch.from_numpy(lig.initpop[:nrun * w["pop"]]).cuda()
+    prng0 = job.prng.clone()
+    res = None
+    for _ in range(args.steps):
+        job.prng.copy_(prng0)
+        res = dock.dock(job, init_dev, args.lsmet, args.nev)
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "loop-kernel", "lsmet": args.lsmet, "nrun": nrun, "nev": args.nev, "dockings": args.steps,
+                      "evals_last": int(res.evals_per_run.sum()), "generations": res.generations,
+                      "docking_loop": dock.last_stats()}))
 
 
 def _ligand_text(config_id, idx, n_heavy, n_tors, types=None):
@@ -729,8 +852,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain sample in the default mode")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving sample in the default mode")
     ap.add_argument("--no-result", action="store_true", help="skip the result-processing sample in the default mode")
-    ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel", "batch", "serve", "result"])
-    ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel mode)")
+    ap.add_argument("--mode", default="dock", choices=["dock", "ls-kernel", "loop-kernel", "batch", "serve", "result"])
+    ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel / loop-kernel modes)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
     ap.add_argument("--engine-tpp", type=int, default=0,
                     help="engine threads per pose (batch / serve modes): 0 = automatic (tuned per ligand size, "
@@ -738,7 +861,7 @@ def main():
     ap.add_argument("--nlig", type=int, default=64, help="ligands (batch mode)")
     ap.add_argument("--batch-config", type=int, default=3, choices=[3, 4],
                     help="batch mode workload: 3 (uneven ligands) or 4 (80^3 maps, 2 flexible residues, nrun 50)")
-    ap.add_argument("--nev", type=int, default=250_000, help="evaluations per run (batch / serve modes)")
+    ap.add_argument("--nev", type=int, default=250_000, help="evaluations per run (batch / serve / loop-kernel modes)")
     ap.add_argument("--plain-sample", type=int, default=16, help="ligands docked one at a time for the plain arm")
     ap.add_argument("--nreq", type=int, default=200, help="requests (serve mode)")
     ap.add_argument("--budget-gb", type=int, default=8, help="engine device-memory budget (serve mode)")
@@ -751,6 +874,9 @@ def main():
     args = ap.parse_args()
     if args.mode == "ls-kernel":
         run_kernel_only(args)
+        return
+    if args.mode == "loop-kernel":
+        run_loop_kernel(args)
         return
     if args.mode in ("batch", "serve", "result"):
         out = {"batch": run_batch, "serve": run_serve, "result": run_result}[args.mode](args)

@@ -524,11 +524,6 @@ adgpu_status adgpu_engine_stats_get(adgpu_engine* engine, adgpu_engine_stats* ou
 /* Threads per pose the engine chose for a request, and its run count. */
 adgpu_status adgpu_engine_request_info(adgpu_engine* engine, uint64_t request_id, int* threads_per_pose, int* runs);
 
-/* Measurement helper (no counterpart in the reference): measured FP32 FMA
- * throughput of the current device in TFLOP/s, the denominator of the
- * scorer's roofline fraction.  device_scratch must hold 2048 floats per SM. */
-adgpu_status adgpu_measure_fp32_peak(float* device_scratch, size_t n_floats, float* tflops);
-
 /* Text of the last error recorded on this thread (never NULL). */
 const char* adgpu_last_error(void);
 
