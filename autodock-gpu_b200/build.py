@@ -87,7 +87,12 @@ def build_probe(force: bool = False, verbose: bool = False) -> str:
 
 
 def build_oracle() -> None:
-    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "-j8"], capture_output=True, text=True)
+    """The oracle libraries; oracle/_ref and the drop-in programs only where the
+    reference checkout is present (ADGPU_REFERENCE, default: the checkout this
+    build was made against)."""
+    ref = os.environ.get("ADGPU_REFERENCE", "/root/reference")
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "-j8", f"REF={ref}"],
+                       capture_output=True, text=True)
     if r.returncode != 0:
         sys.stdout.write(r.stdout)
         sys.stderr.write(r.stderr)

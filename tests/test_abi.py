@@ -72,3 +72,21 @@ def test_errors_without_set_data():
     st = L.adgpu_sum_evals(1, 64)
     assert st == 3
     assert b"not called" in L.adgpu_last_error()
+
+
+DROPIN = os.path.join(ROOT, "oracle", "_ref", "autodock_gpu_b200")
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN), reason="reference host program not built (make -C oracle dropin)")
+def test_reference_host_program_binds_the_library():
+    """The reference's host program, built from its own sources, takes the
+    kernel API from libadgpu_b200.so: the seven kernel-API names are
+    undefined in the program and resolve to this library."""
+    und = subprocess.run(["nm", "-D", "--undefined-only", DROPIN], capture_output=True, text=True).stdout
+    for s in REFERENCE_CXX_SYMBOLS:
+        if s.startswith("_Z17GetKernelsGpuData"):
+            continue            # the host program never calls it
+        assert s in und, s
+    deps = subprocess.run(["ldd", DROPIN], capture_output=True, text=True).stdout
+    assert os.path.realpath(lib.LIB_PATH) in {os.path.realpath(p.split("=>")[1].split("(")[0].strip())
+                                              for p in deps.splitlines() if "libadgpu_b200" in p}
