@@ -136,7 +136,8 @@ class DockStats(C.Structure):
     """adgpu_dock_stats: accounting of the last adgpu_dock_resident call."""
     _fields_ = [("pipelined", C.c_int), ("threads_per_pose", C.c_int), ("pose_groups", C.c_int),
                 ("generations", C.c_uint32), ("generations_discarded", C.c_uint32), ("tasks", C.c_uint64),
-                ("parks", C.c_uint64), ("busy_s", C.c_double), ("span_s", C.c_double)]
+                ("parks", C.c_uint64), ("evals_executed", C.c_uint64), ("buffers", C.c_int), ("pad", C.c_int),
+                ("busy_s", C.c_double), ("span_s", C.c_double)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_}

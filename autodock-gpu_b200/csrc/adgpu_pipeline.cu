@@ -13,16 +13,23 @@
 // Here every run's generation is split into one task per entity -- the GA
 // step that makes the entity (elitism, or tournaments, crossover, mutation
 // and scoring) followed by its local search, both on the entity's own PRNG
-// states in the reference's order -- on one device task ring, and a run
-// starts its next generation as soon as its own last task ends.  The stop
+// states in the reference's order -- and a run starts its next generation as
+// soon as its own last task ends.  Each run hands out the entities of its
+// current generation from one counter (generation << 32 | entities taken);
+// a pose group scans the runs' counters and takes an entity of a run in the
+// oldest open generation, so the runs that gate the next stop test are never
+// queued behind runs that are ahead of them.  The stop
 // test keeps the reference's semantics exactly: check g (before generation g)
 // uses the evaluations of all runs after generation g-1, so it is taken by
 // whichever pose group completes the last run's generation g-1.  Runs may
-// run ahead of that decision by up to kPipeBufs-1 generations: generation g
-// reads population buffer g % kPipeBufs and writes buffer (g+1) % kPipeBufs,
-// which holds the result of generation g - kPipeBufs; that result is needed
-// only if check g - kPipeBufs + 1 says stop, so generation g may start once
-// that check has said continue.  When a check says stop, the generations
+// run ahead of that decision by up to nbuf-1 generations (nbuf population
+// buffers, 4 or 8): generation g reads buffer g % nbuf and writes buffer
+// (g+1) % nbuf, which holds the result of generation g - nbuf; that result is
+// needed only if check g - nbuf + 1 says stop, so generation g may start once
+// that check has said continue.  Generations the evaluation count will not
+// reach are not started: each check projects the generation at which the
+// stop will come from the evaluations the last generation added, and runs
+// wait at one generation past it until the next check.  When a check says stop, the generations
 // already run past it are discarded: their evaluations are taken back off the
 // per-run counters and the final population is the one the reference ends
 // with.  Every run performs exactly the reference's operations on its own
@@ -32,6 +39,7 @@
 // to the generation-synchronous loop; only the PRNG states and the per-entity
 // evaluation counters of the discarded generations differ.
 #include <cuda_runtime.h>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -46,35 +54,37 @@
 namespace adgpu {
 
 constexpr int kPipeThreads = 128;
-constexpr uint32_t kPipeRunShift = 11;         // task word: run << 11 | entity
-constexpr uint32_t kPipeStop = 0x7fffffffu;    // task word that ends a worker
+constexpr uint32_t kPipeRunShift = 11;         // a taken task: run << 11 | entity
 constexpr int kRetired = 0x40000000;           // started[r] of a retired run
 
-__host__ __device__ constexpr uint32_t pipe_word(uint32_t run, uint32_t entity)
-{
-	return (run << kPipeRunShift) | entity;
-}
 
 struct PipeCtl {
-	QueueCtl q;                               // ring control; q.alive = runs not retired
+	QueueCtl q;                               // q.alive = runs not retired, q.err, accounting
+	int done;                                 // every run has retired
 	int dec;                                  // checks 0 .. dec-1 have said continue
 	int stop_gen;                             // -1, or the generations run (the check that said stop)
 	unsigned long long parks;                 // times a run waited for a check before its next generation
+	unsigned long long executed;              // evaluations executed, discarded generations included
+	unsigned long long last_tot;              // evaluations over all runs at the last check
+	int limit;                                // generations above this one do not start (projected stop)
+	int pad;
 	unsigned long long acc[kPipeBufs];        // per generation slot: sum over runs of the evaluations after it
 	int fin[kPipeBufs];                       // per generation slot: runs that completed it
 };
 
 struct PipeArgs {
 	KArgs ka;                   // tables, dockpars, PRNG states, evaluation counters
-	PopBufs bufs[kPipeBufs];    // generation slot k: conf_cur/e_cur = buffer k, conf/e = buffer k+1
-	TaskRing ring;
+	PopBufs bufs[kPipeBufs];    // generation slot k: conf_cur/e_cur = buffer k, conf/e = buffer (k+1) % nbuf
+	unsigned long long* next;   // R: the run's open generation << 32 | its entities taken
+	long long idle_ns;          // a pose group that finds no task for this long gives up (error)
 	PipeCtl* ctl;
 	int* started;               // R: generations started (claimed), kRetired once retired
 	int* done;                  // R: generations completed (or abandoned after a stop)
 	int* comp;                  // R: generations whose evaluations are in evals_runs
 	int* pending;               // R: tasks of the run's current phase not yet finished
 	int* inc;                   // R * kPipeBufs: evaluations each generation slot added
-	int runs, pop, nworkers;
+	int runs, pop;
+	int nbuf;                   // population buffers in use (4 or 8): look-ahead nbuf-1 generations
 	unsigned long long max_evals;
 	unsigned int max_gens;
 	int group_bytes;            // shared memory per pose group (header + scratch)
@@ -83,7 +93,7 @@ struct PipeArgs {
 struct PipeHdr {
 	unsigned long long pos;
 	long long t_enter, t_task;       // worker accounting (rank 0; globaltimer ns)
-	unsigned long long busy, ntask;
+	unsigned long long busy, ntask, nevals;
 	int task, gen, last, decider, stopped, isum;
 };
 constexpr int kPipeHdrBytes = (int)((sizeof(PipeHdr) + 15) / 16 * 16);
@@ -101,18 +111,74 @@ __device__ void pipe_try_start(const PipeArgs& p, int r)
 	volatile PipeCtl* vc = p.ctl;
 	if (vc->stop_gen >= 0) {
 		// the last run to retire ends every worker
-		if (atomicCAS(p.started + r, d, kRetired) == d && atomicSub(&p.ctl->q.alive, 1) == 1)
-			ring_push_n(p.ring, kPipeStop, p.nworkers);
+		if (atomicCAS(p.started + r, d, kRetired) == d && atomicSub(&p.ctl->q.alive, 1) == 1) {
+			__threadfence();
+			vc->done = 1;
+		}
 		return;
 	}
-	if (d - kPipeBufs + 1 >= vc->dec) {               // parked: check d-kPipeBufs+1 still open
+	if (d - p.nbuf + 1 >= vc->dec || d > vc->limit) { // parked: check d-nbuf+1 still open, or past the projected stop
 		atomicAdd(&p.ctl->parks, 1ull);
 		return;
 	}
 	if (atomicCAS(p.started + r, d, d + 1) != d) return;
 	p.pending[r] = p.pop;
 	__threadfence();
-	ring_push1(p.ring, pipe_word((uint32_t)r, 0), p.pop);
+	// open generation d's entities
+	atomicExch(p.next + r, (unsigned long long)d << 32);
+}
+
+// An entity to work on: the first warp of the pose group scans the runs'
+// counters for the lowest open generation with entities left (ties: the
+// first run at or after this group's own offset, so that groups spread over
+// the runs), and takes one with an atomicAdd; a take past the run's last
+// entity only sends the scan round again.  Returns run << 11 | entity and the
+// generation in *gen, or -1 once every run has retired (or after idle_ns with
+// nothing to take: an error).
+template <int TPP>
+__device__ int pipe_take(const PipeArgs& p, int worker, const Group<TPP>& G, int* gen)
+{
+	volatile PipeCtl* vc = p.ctl;
+	const int lane = G.rank;            // called by the group's first warp only
+	const int R = p.runs, P = p.pop;
+	const int off = worker % R;
+	long long idle_since = -1;
+	int backoff = 64;
+	for (int spins = 0; spins < (1 << 30); spins++) {
+		if (vc->done) return -1;
+		unsigned long long best = ~0ull;
+		for (int r = lane; r < R; r += 32) {
+			const unsigned long long v = *reinterpret_cast<const volatile unsigned long long*>(p.next + r);
+			if ((uint32_t)v < (uint32_t)P) {
+				const unsigned long long key = ((v >> 32) << 32) | (uint32_t)((r - off + R) % R);
+				best = key < best ? key : best;
+			}
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
+			best = x < best ? x : best;
+		}
+		if (best != ~0ull) {
+			const int r = (int)(((uint32_t)best + off) % (uint32_t)R);
+			unsigned long long old = 0;
+			if (lane == 0) old = atomicAdd(p.next + r, 1ull);
+			old = __shfl_sync(0xffffffffu, old, 0);
+			if ((uint32_t)old < (uint32_t)P) {
+				__threadfence();
+				*gen = (int)(old >> 32);
+				return (r << kPipeRunShift) | (int)(uint32_t)old;
+			}
+			continue;
+		}
+		const long long now = global_ns();
+		if (idle_since < 0) idle_since = now;
+		else if (now - idle_since > p.idle_ns) break;
+		__nanosleep(backoff);
+		if (backoff < 4096) backoff *= 2;
+	}
+	if (lane == 0) atomicExch(&p.ctl->q.err, 2);
+	return -1;
 }
 
 template <int TPP, int LSMET>
@@ -129,16 +195,18 @@ __device__ void pipe_worker(const PipeArgs& p)
 	G.bar_id = 1 + local;
 	G.red = S.red;
 	const int P = p.pop, R = p.runs;
-	if (G.rank == 0) { H.t_enter = global_ns(); H.t_task = 0; H.busy = 0; H.ntask = 0; }
+	if (G.rank == 0) { H.t_enter = global_ns(); H.t_task = 0; H.busy = 0; H.ntask = 0; H.nevals = 0; }
+	const int worker = blockIdx.x * (kPipeThreads / TPP) + local;
 	for (;;) {
-		if (G.rank == 0) {
-			if (H.t_task) H.busy += (unsigned long long)(global_ns() - H.t_task);
-			const int w = ring_take(p.ring);
-			H.task = (w < 0 || (uint32_t)w == kPipeStop) ? -1 : w;
-			H.t_task = H.task >= 0 ? global_ns() : 0;
-			H.ntask += H.task >= 0;
-			if (H.task >= 0) {
-				H.gen = vload(p.started + (H.task >> kPipeRunShift)) - 1;
+		if (G.rank < 32) {
+			if (G.rank == 0 && H.t_task) H.busy += (unsigned long long)(global_ns() - H.t_task);
+			int gen = 0;
+			const int task = pipe_take<TPP>(p, worker, G, &gen);
+			if (G.rank == 0) {
+				H.task = task;
+				H.t_task = task >= 0 ? global_ns() : 0;
+				H.ntask += task >= 0;
+				H.gen = gen;
 				H.stopped = reinterpret_cast<volatile PipeCtl*>(p.ctl)->stop_gen >= 0;
 			}
 		}
@@ -152,7 +220,7 @@ __device__ void pipe_worker(const PipeArgs& p)
 		// only count down
 		if (!H.stopped) {
 			const KArgs& a = p.ka;
-			const PopBufs pb = p.bufs[g & (kPipeBufs - 1)];
+			const PopBufs pb = p.bufs[g & (p.nbuf - 1)];
 			const uint32_t b = (uint32_t)(run * P + ent);
 			ga_block<TPP>(a, pb, b, G, S);
 			// num_of_lsentities == pop_size: local-search block b is entity b
@@ -163,7 +231,10 @@ __device__ void pipe_worker(const PipeArgs& p)
 		}
 		__threadfence();
 		G.sync();
-		if (G.rank == 0) H.last = (atomicSub(p.pending + run, 1) == 1);
+		if (G.rank == 0) {
+			if (!H.stopped) H.nevals += (unsigned long long)p.ka.evals_new[run * P + ent];
+			H.last = (atomicSub(p.pending + run, 1) == 1);
+		}
 		G.sync();
 		if (!H.last) continue;
 		__threadfence();
@@ -182,7 +253,7 @@ __device__ void pipe_worker(const PipeArgs& p)
 		}
 		if (G.rank == 0) {
 			H.decider = 0;
-			const int slot = g & (kPipeBufs - 1);
+			const int slot = g & (p.nbuf - 1);
 			if (!H.stopped) {
 				// the eval sum of the run (cuda/kernel2.cu:26-52)
 				int* er = p.ka.evals_runs + run;
@@ -205,8 +276,21 @@ __device__ void pipe_worker(const PipeArgs& p)
 					// a generation run past a stop can still complete everywhere
 					// (its last tasks were taken before the stop was seen)
 					if (vc->stop_gen < 0) {
-						if ((ev > gp ? ev : gp) >= 100.0) vc->stop_gen = g + 1;
-						else vc->dec = g + 2;
+						if ((ev > gp ? ev : gp) >= 100.0) {
+							vc->stop_gen = g + 1;
+						} else {
+							// project the stop: generations g+1 .. g+k still to run
+							// at the rate generation g added; start none past g+k+1
+							const unsigned long long target = (unsigned long long)R * p.max_evals;
+							const unsigned long long delta = tot > p.ctl->last_tot ? tot - p.ctl->last_tot : 1ull;
+							const unsigned long long k = (target - tot + delta - 1) / delta;
+							long long lim = (long long)g + (long long)k + 1;
+							if (lim > (long long)p.max_gens - 1) lim = (long long)p.max_gens - 1;
+							if (lim > 0x3fffffff) lim = 0x3fffffff;
+							vc->limit = (int)lim;
+							p.ctl->last_tot = tot;
+							vc->dec = g + 2;
+						}
 					}
 					H.decider = 1;
 				}
@@ -225,6 +309,7 @@ __device__ void pipe_worker(const PipeArgs& p)
 	}
 	if (G.rank == 0) {
 		atomicAdd(&p.ctl->q.busy_ns, H.busy);
+		atomicAdd(&p.ctl->executed, H.nevals);
 		atomicAdd(&p.ctl->q.tasks, H.ntask);
 		atomicAdd(&p.ctl->q.workers, 1);
 		atomicMin(&p.ctl->q.t_first, (unsigned long long)H.t_enter);
@@ -255,28 +340,22 @@ __global__ void __launch_bounds__(256) pipe_init_kernel(PipeArgs p)
 		p.done[r] = 0;
 		p.comp[r] = 0;
 		p.pending[r] = p.pop;
-		if (!stop)
-			for (int e = 0; e < p.pop; e++) {
-				const unsigned long long pos = (unsigned long long)r * p.pop + e;
-				p.ring.slots[pos] = (1ull << 32) | pipe_word((uint32_t)r, (uint32_t)e);
-			}
+		p.next[r] = stop ? (unsigned long long)(uint32_t)p.pop : 0ull;   // generation 0 open, or nothing to take
 	}
-	// nothing to run: one stop word per worker
-	if (stop)
-		for (int i = threadIdx.x; i < p.nworkers; i += blockDim.x) p.ring.slots[i] = (1ull << 32) | kPipeStop;
 	if (threadIdx.x == 0) {
 		PipeCtl* c = p.ctl;
-		c->q.head = 0;
-		c->q.tail = stop ? (unsigned long long)p.nworkers : (unsigned long long)p.runs * p.pop;
 		c->q.alive = stop ? 0 : p.runs;
+		c->done = stop ? 1 : 0;
 		c->dec = 1;
 		c->stop_gen = stop ? 0 : -1;
 		c->q.t_first = ~0ull;
+		c->last_tot = tot;
+		c->limit = (int)(p.max_gens - 1 < 0x3fffffffu ? p.max_gens - 1 : 0x3fffffffu);
 	}
 }
 
 // Takes the evaluations of discarded generations back off the per-run
-// counters.  out: generations run, runs not retired, ring error, most
+// counters.  out: generations run, runs not retired, task error, most
 // generations a run ran past the stop, then the accounting (busy ns, tasks,
 // first start, last exit, parks, pose groups).
 __global__ void __launch_bounds__(256) pipe_final_kernel(PipeArgs p, long long* out)
@@ -287,7 +366,7 @@ __global__ void __launch_bounds__(256) pipe_final_kernel(PipeArgs p, long long* 
 	const int G = p.ctl->stop_gen;
 	for (int r = threadIdx.x; r < p.runs; r += blockDim.x)
 		if (G >= 0) {
-			for (int k = G; k < p.comp[r]; k++) p.ka.evals_runs[r] -= p.inc[r * kPipeBufs + (k & (kPipeBufs - 1))];
+			for (int k = G; k < p.comp[r]; k++) p.ka.evals_runs[r] -= p.inc[r * kPipeBufs + (k & (p.nbuf - 1))];
 			atomicMax(&past, p.done[r] - G);
 		}
 	__syncthreads();
@@ -296,7 +375,7 @@ __global__ void __launch_bounds__(256) pipe_final_kernel(PipeArgs p, long long* 
 		out[0] = G; out[1] = q.alive; out[2] = q.err; out[3] = past;
 		out[4] = (long long)q.busy_ns; out[5] = (long long)q.tasks;
 		out[6] = q.workers ? (long long)(q.t_last - q.t_first) : 0;
-		out[7] = (long long)p.ctl->parks; out[8] = q.workers;
+		out[7] = (long long)p.ctl->parks; out[8] = q.workers; out[9] = (long long)p.ctl->executed;
 	}
 }
 
@@ -320,7 +399,6 @@ static adgpu_status launch_pipe(PipeArgs p, long long* d_out, cudaStream_t st)
 	const long useful = ((long)p.runs * p.pop + gpc - 1) / gpc;
 	long grid = (long)per_sm * sms;
 	if (grid > useful) grid = useful;
-	p.nworkers = (int)grid * gpc;
 	pipe_init_kernel<<<1, 256, 0, st>>>(p);
 	ADGPU_CUDA_RET(cudaGetLastError(), "pipeline init");
 	kfn<<<(int)grid, kPipeThreads, bytes, st>>>(p);
@@ -336,18 +414,30 @@ bool pipeline_applies(const adgpu_dockpars& dp, uint32_t runs)
 	       dp.pop_size <= (1 << kPipeRunShift) && runs > 0 && runs < (1u << (31 - kPipeRunShift));
 }
 
-// Threads per pose of the pipelined loop.  Solis-Wets and ADADELTA: 64.
-// Their searches stop on their own test (cfg2 ADADELTA: mean 67, up to 300
-// iterations), so a run's generation lasts as long as its longest search, and
-// with 32 threads per pose that chain of generations, not the pose groups'
-// throughput, sets the docking time (B200, cfg2 ADADELTA, 100 runs: 64
-// threads 150 M evals/s with the pose groups 99 % busy, 32 threads 140 M at
-// 81 % busy).  ADAM and FIRE run a fixed iteration count, so a generation
-// holds far more work than its longest chain: 32, the group size with the
-// higher throughput.
+// Threads per pose of the pipelined loop: 32 for every local search.  Runs
+// advance independently and a generation's entities are handed out oldest
+// generation first, so the launch no longer ends each generation with its
+// longest searches running alone (the reason the per-generation launches use
+// 64 for Solis-Wets and ADADELTA), and one warp per pose gives the most
+// evaluations per SM (B200, cfg2, 100 runs: ADADELTA 158 vs 148, Solis-Wets
+// 255 vs 249, ADAM 174 vs 155, FIRE 140 vs 119 M evals/s against 64).
 int pipeline_default_tpp(int lsmet)
 {
-	return (lsmet == 0 || lsmet == 1) ? 64 : 32;
+	(void)lsmet;
+	return 32;
+}
+
+// Population buffers (look-ahead + 1): with 32 threads per pose a run's
+// generation takes longer (its longest search runs on one warp), so runs are
+// let further ahead of the slowest (ADADELTA: pose groups 94 % busy with 8
+// buffers, 94 % with 4; with 64 threads 99 % either way).
+int pipeline_buffers(int tpp)
+{
+	if (const char* e = getenv("ADGPU_PIPELINE_BUFFERS")) {
+		const int v = atoi(e);
+		if (v == 4 || v == 8) return v;
+	}
+	return tpp == 32 ? 8 : 4;
 }
 
 adgpu_status dock_pipelined(const KArgs& base, PipeScratch& sc, int lsmet, int tpp, uint32_t runs,
@@ -360,19 +450,13 @@ adgpu_status dock_pipelined(const KArgs& base, PipeScratch& sc, int lsmet, int t
 	if (tpp != 32 && tpp != 64 && tpp != 128) return fail(ADGPU_ERR_ARG, "threads per pose must be 32, 64 or 128");
 	const int P = dp.pop_size;
 	const size_t n = (size_t)runs * P;
-	// in flight at once: at most one generation's tasks per run, plus one
-	// claimed position and one stop word per worker (at most 148 SMs x 32
-	// pose groups here; the device's count is checked below)
-	int dev = 0, sms = 0;
-	ADGPU_CUDA_RET(cudaGetDevice(&dev), "device");
-	ADGPU_CUDA_RET(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
-	const size_t max_workers = (size_t)sms * 2048 / 32;
-	const size_t cap = 2 * ((size_t)runs * P + 2 * max_workers) + 1024;
-	// scratch: two more population buffers, the ring, per-run counters, control
+	const int nbuf = pipeline_buffers(tpp);
+	// scratch: nbuf-2 more population buffers, per-run counters, control
 	auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-	const size_t o_conf = 0, conf_b = al(n * kGenotypeStride * 4) * 2;
-	const size_t o_e = o_conf + conf_b, e_b = al(n * 4) * 2;
-	const size_t o_slots = o_e + e_b, slots_b = al(cap * 8);
+	const size_t conf1 = al(n * kGenotypeStride * 4), e1b = al(n * 4);
+	const size_t o_conf = 0, conf_b = conf1 * (nbuf - 2);
+	const size_t o_e = o_conf + conf_b, e_b = e1b * (nbuf - 2);
+	const size_t o_slots = o_e + e_b, slots_b = al((size_t)runs * 8);
 	const size_t o_runs = o_slots + slots_b, runs_b = al((size_t)runs * 4) * 4 + al((size_t)runs * kPipeBufs * 4);
 	const size_t o_ctl = o_runs + runs_b, ctl_b = al(sizeof(PipeCtl)) + 256;
 	const size_t total = o_ctl + ctl_b;
@@ -384,8 +468,12 @@ adgpu_status dock_pipelined(const KArgs& base, PipeScratch& sc, int lsmet, int t
 	}
 	if (!sc.host_out) ADGPU_CUDA_RET(cudaMallocHost(&sc.host_out, 16 * sizeof(long long)), "pipeline readback");
 	char* m = static_cast<char*>(sc.mem);
-	float* conf[kPipeBufs] = {c1, c2, reinterpret_cast<float*>(m + o_conf), reinterpret_cast<float*>(m + o_conf + conf_b / 2)};
-	float* en[kPipeBufs] = {e1, e2, reinterpret_cast<float*>(m + o_e), reinterpret_cast<float*>(m + o_e + e_b / 2)};
+	float* conf[kPipeBufs] = {c1, c2};
+	float* en[kPipeBufs] = {e1, e2};
+	for (int k = 2; k < nbuf; k++) {
+		conf[k] = reinterpret_cast<float*>(m + o_conf + conf1 * (k - 2));
+		en[k] = reinterpret_cast<float*>(m + o_e + e1b * (k - 2));
+	}
 	PipeArgs p;
 	memset(&p, 0, sizeof(p));
 	p.ka = base;
@@ -395,17 +483,15 @@ adgpu_status dock_pipelined(const KArgs& base, PipeScratch& sc, int lsmet, int t
 	p.ka.nblocks = 0;
 	p.ka.conf_cur = p.ka.e_cur = nullptr;
 	p.ka.conf = p.ka.e = nullptr;
-	for (int k = 0; k < kPipeBufs; k++)
-		p.bufs[k] = PopBufs{conf[k], en[k], conf[(k + 1) % kPipeBufs], en[(k + 1) % kPipeBufs]};
-	p.ring.slots = reinterpret_cast<unsigned long long*>(m + o_slots);
-	p.ring.cap = (uint32_t)cap;
-	p.ring.slot_spin = 1 << 20;     // (ring_take bounds its wait by idle_ns)
-	p.ring.idle_ns = 2000000000ll;
+	p.nbuf = nbuf;
+	for (int k = 0; k < nbuf; k++)
+		p.bufs[k] = PopBufs{conf[k], en[k], conf[(k + 1) % nbuf], en[(k + 1) % nbuf]};
+	p.next = reinterpret_cast<unsigned long long*>(m + o_slots);
+	p.idle_ns = 2000000000ll;
 	int* ri = reinterpret_cast<int*>(m + o_runs);
 	const size_t rs = al((size_t)runs * 4) / 4;
 	p.started = ri; p.done = ri + rs; p.comp = ri + 2 * rs; p.pending = ri + 3 * rs; p.inc = ri + 4 * rs;
 	p.ctl = reinterpret_cast<PipeCtl*>(m + o_ctl);
-	p.ring.ctl = &p.ctl->q;
 	long long* d_out = reinterpret_cast<long long*>(m + o_ctl + al(sizeof(PipeCtl)));
 	p.runs = (int)runs; p.pop = P;
 	p.max_evals = max_evals; p.max_gens = max_gens;
@@ -416,7 +502,6 @@ adgpu_status dock_pipelined(const KArgs& base, PipeScratch& sc, int lsmet, int t
 	// second buffer: genes past num_of_genes are never written
 	ADGPU_CUDA_RET(cudaMemsetAsync(m + o_conf, 0, conf_b + e_b, st), "pipeline buffers");
 	ADGPU_CUDA_RET(cudaMemsetAsync(p.ctl, 0, sizeof(PipeCtl), st), "pipeline control");
-	ADGPU_CUDA_RET(cudaMemsetAsync(p.ring.slots, 0, cap * 8, st), "pipeline ring");
 	adgpu_status rc = ADGPU_OK;
 #define ADGPU_PIPE_LSMET(T) \
 	switch (lsmet) { \
@@ -432,7 +517,7 @@ adgpu_status dock_pipelined(const KArgs& base, PipeScratch& sc, int lsmet, int t
 	}
 #undef ADGPU_PIPE_LSMET
 	if (rc != ADGPU_OK) return rc;
-	ADGPU_CUDA_RET(cudaMemcpyAsync(sc.host_out, d_out, 9 * sizeof(long long), cudaMemcpyDeviceToHost, st), "pipeline readback");
+	ADGPU_CUDA_RET(cudaMemcpyAsync(sc.host_out, d_out, 10 * sizeof(long long), cudaMemcpyDeviceToHost, st), "pipeline readback");
 	ADGPU_CUDA_RET(cudaStreamSynchronize(st), "pipeline docking");
 	const long long* o = sc.host_out;
 	const int G = (int)o[0], alive = (int)o[1], err = (int)o[2];
@@ -447,12 +532,14 @@ adgpu_status dock_pipelined(const KArgs& base, PipeScratch& sc, int lsmet, int t
 	ds.tasks = (uint64_t)o[5];
 	ds.span_s = 1e-9 * (double)o[6];
 	ds.parks = (uint64_t)o[7];
+	ds.evals_executed = (uint64_t)o[9];
+	ds.buffers = nbuf;
 	if (err != 0 || alive != 0 || G < 0)
-		return fail(ADGPU_ERR_TIMEOUT, "pipelined docking: a bounded device wait gave up (ring error " + std::to_string(err) +
+		return fail(ADGPU_ERR_TIMEOUT, "pipelined docking: a bounded device wait gave up (task error " + std::to_string(err) +
 		                                ", runs still active " + std::to_string(alive) + ")");
 	*generations = (uint32_t)G;
 	*final_is_second = G & 1;
-	const int fb = G & (kPipeBufs - 1);
+	const int fb = G & (nbuf - 1);
 	if (fb >= 2) {
 		// the final population sits in a library buffer: copy it to the
 		// caller's buffer the synchronous loop would have left it in

@@ -10,9 +10,10 @@
 
 namespace adgpu {
 
-// Population buffers of the pipelined loop: the caller's two plus two of the
-// library's; runs may run up to kPipeBufs-1 generations ahead of the stop test.
-constexpr int kPipeBufs = 4;
+// Most population buffers of the pipelined loop (the caller's two plus the
+// library's); with nbuf of them runs may run up to nbuf-1 generations ahead
+// of the stop test.
+constexpr int kPipeBufs = 8;
 
 // Library-owned device scratch of the pipelined loop, kept between calls.
 struct PipeScratch {

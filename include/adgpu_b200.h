@@ -307,6 +307,9 @@ typedef struct {
 	uint32_t generations_discarded;   /* most generations any run ran past the stop */
 	uint64_t tasks;                   /* GA chunks and local searches executed */
 	uint64_t parks;                   /* times a run waited for a stop test before its next generation */
+	uint64_t evals_executed;          /* evaluations executed, those of discarded generations included */
+	int      buffers;                 /* population buffers (look-ahead + 1 generations) */
+	int      pad;
 	double   busy_s;                  /* summed time pose groups spent on tasks */
 	double   span_s;                  /* first pose group start to last pose group exit */
 } adgpu_dock_stats;
