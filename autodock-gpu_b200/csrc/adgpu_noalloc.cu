@@ -4,9 +4,8 @@
 // tables and its cell-record grid, which adgpu_set_kernels_gpu_data
 // allocates with cudaMalloc.  Some callers cannot allocate at all: a host
 // that owns all device memory through its own pool and forbids foreign
-// allocations, code that scores poses while the device is being captured
-// into a graph (cudaMalloc is not a capturable operation), or a process
-// whose memory is already fully reserved.  For them,
+// allocations, or a process whose device memory is already fully reserved.
+// For them,
 // adgpu_score_genotypes_noalloc repacks the caller's reference-layout tables
 // on the device into one fixed, file-scope device array and reads the
 // caller's grid in its own layout, so the only memory it touches besides its
@@ -97,6 +96,12 @@ __global__ void __launch_bounds__(256) noalloc_repack_kernel(adgpu_gpudata d, Li
 		s_start[a + 1] = cnt;
 		clen[a] = (uint8_t)cnt;
 		info[a] = genrot ? 0x200u : 0u;
+	}
+	// a rotation-list entry must name one of the atoms (the repack on the
+	// host rejects the same, adgpu_tables.cu)
+	for (int k = threadIdx.x; k < dp.rotbondlist_length; k += blockDim.x) {
+		const int el = rl[k];
+		if (!(el & ADGPU_RLIST_DUMMY_MASK) && (el & ADGPU_RLIST_ATOMID_MASK) >= N) status[0] = 1;
 	}
 	__syncthreads();
 	if (threadIdx.x == 0) {
@@ -228,7 +233,8 @@ extern "C" adgpu_status adgpu_score_genotypes_noalloc(const adgpu_gpudata* data,
 	    dp.num_of_intraE_contributors < 0 || dp.num_of_intraE_contributors > ADGPU_MAX_INTRAE ||
 	    dp.rotbondlist_length < 0 || dp.rotbondlist_length > ADGPU_MAX_ROTATIONS || dp.num_of_atypes <= 0 ||
 	    dp.num_of_atypes > ADGPU_MAX_ATYPES || dp.true_ligand_atoms < 0 || dp.true_ligand_atoms > dp.num_of_atoms ||
-	    dp.num_of_map_atypes <= 0 || dp.gridsize_x < 2 || dp.gridsize_y < 2 || dp.gridsize_z < 2)
+	    dp.num_of_map_atypes <= 0 || dp.num_of_map_atypes > ADGPU_MAX_ATYPES ||
+	    dp.gridsize_x < 2 || dp.gridsize_y < 2 || dp.gridsize_z < 2)
 		return fail(ADGPU_ERR_LIMIT, "docking parameters out of the reference's limits");
 	const NoAllocLayout lay = layout_for(dp);
 	if (lay.total > kNoAllocScratchBytes)
@@ -293,7 +299,8 @@ extern "C" adgpu_status adgpu_score_genotypes_noalloc(const adgpu_gpudata* data,
 	k<<<grid, 128, bytes>>>(lay.ligdev, dp, n, genotypes, energies, gradients);
 	e = cudaGetLastError();
 	if (e != cudaSuccess) return cuda_fail(e, "score launch");
-	e = cudaDeviceSynchronize();
+	// both kernels ran on the legacy default stream: wait for them only
+	e = cudaStreamSynchronize(cudaStreamLegacy);
 	if (e != cudaSuccess) return cuda_fail(e, "score");
 	return ADGPU_OK;
 }

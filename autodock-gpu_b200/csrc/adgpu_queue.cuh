@@ -1,5 +1,5 @@
-// adgpu_queue.cuh -- the device task ring shared by the persistent kernels
-// (the batch/serving engine and the pipelined plain docking loop).
+// adgpu_queue.cuh -- the device task ring of the batch/serving engine's
+// persistent kernel, and the globaltimer read the persistent kernels share.
 //
 // A ring of 64-bit slots: a producer reserves positions with one atomicAdd on
 // `tail` and writes each slot as (lap << 32) | task word, lap = position / cap
@@ -74,57 +74,6 @@ __device__ inline int ring_pop(const TaskRing& C, long long deadline)
 	}
 	atomicExch(&C.ctl->err, 2);
 	return -1;
-}
-
-// Ticket pop for rings whose consumers never stop early: claims the next
-// position with one atomicAdd and waits for its slot (idle workers poll their
-// own slots, not one shared word).  Returns the task word, or -1 (ctl->err
-// set) when the slot stayed unwritten for idle_ns.  Every claimed position
-// must eventually be written: a producer ends the ring by pushing one stop
-// word per consumer.
-__device__ inline int ring_take(const TaskRing& C)
-{
-	const unsigned long long h = atomicAdd(&C.ctl->head, 1ull);
-	const unsigned long long want = h / C.cap + 1;
-	volatile unsigned long long* s = C.slots + (h % C.cap);
-	long long since = -1;
-	for (int k = 0; k < (1 << 30); k++) {
-		const unsigned long long v = *s;
-		if ((v >> 32) == want) {
-			__threadfence();
-			return (int)(uint32_t)v;
-		}
-		if ((k & 31) == 31) {
-			const long long now = global_ns();
-			if (since < 0) since = now;
-			else if (now - since > C.idle_ns) break;
-		}
-		__nanosleep(k < 32 ? 32 : 256);
-	}
-	atomicExch(&C.ctl->err, 1);
-	return -1;
-}
-
-// Pushes n copies of `word` from one thread.
-__device__ inline void ring_push_n(const TaskRing& C, uint32_t word, int n)
-{
-	const unsigned long long p0 = atomicAdd(&C.ctl->tail, (unsigned long long)n);
-	__threadfence();
-	for (int i = 0; i < n; i++) {
-		const unsigned long long p = p0 + (unsigned long long)i;
-		atomicExch(C.slots + (p % C.cap), ((p / C.cap + 1) << 32) | word);
-	}
-}
-
-// Pushes task words word0 | i, i in [0, n), from one thread.
-__device__ inline void ring_push1(const TaskRing& C, uint32_t word0, int n)
-{
-	const unsigned long long p0 = atomicAdd(&C.ctl->tail, (unsigned long long)n);
-	__threadfence();
-	for (int i = 0; i < n; i++) {
-		const unsigned long long p = p0 + (unsigned long long)i;
-		atomicExch(C.slots + (p % C.cap), ((p / C.cap + 1) << 32) | (word0 | (uint32_t)i));
-	}
 }
 
 // Pushes task words word0 | i, i in [0, n), with a whole pose group; `pos` is

@@ -229,6 +229,14 @@ adgpu_status adgpu_gradient_minfire(uint32_t blocks, uint32_t threads,
 adgpu_status adgpu_score_genotypes(uint32_t n, const float* genotypes,
                                    float* energies, float* gradients);
 
+/* The scorer's energy split into its terms, for n genotypes (device
+ * buffers; no reference counterpart, the parity tests' per-term view):
+ * energies[n], and terms[8n] per genotype = intermolecular type-map,
+ * electrostatic and desolvation energies, intramolecular vdW/H-bond,
+ * electrostatic, desolvation and CG-G0 energies, and the number of atoms
+ * outside the grid (each adds the 2^24 penalty to the energy only). */
+adgpu_status adgpu_score_terms(uint32_t n, const float* genotypes, float* energies, float* terms);
+
 /* The same scoring as adgpu_score_genotypes, for callers that may not
  * allocate device memory: a host whose memory is all handed out by its own
  * pool, or a process with every byte of the device already reserved.  It has
@@ -241,16 +249,8 @@ adgpu_status adgpu_score_genotypes(uint32_t n, const float* genotypes,
  * on a device looks up that array's device address (cudaGetSymbolAddress),
  * so make it before any stream capture.  There is one array per device:
  * calls that overlap on the GPU (from several host threads) race on it.
- * Runs on the legacy default stream and returns after the scores are
- * written. */
-/* The scorer's energy split into its terms, for n genotypes (device
- * buffers; no reference counterpart, the parity tests' per-term view):
- * energies[n], and terms[8n] per genotype = intermolecular type-map,
- * electrostatic and desolvation energies, intramolecular vdW/H-bond,
- * electrostatic, desolvation and CG-G0 energies, and the number of atoms
- * outside the grid (each adds the 2^24 penalty to the energy only). */
-adgpu_status adgpu_score_terms(uint32_t n, const float* genotypes, float* energies, float* terms);
-
+ * Runs on the legacy default stream and returns once its own kernels have
+ * finished (it synchronises that stream, not the whole device). */
 adgpu_status adgpu_score_genotypes_noalloc(const adgpu_gpudata* data, uint32_t n,
                                            const float* genotypes, float* energies,
                                            float* gradients);

@@ -57,6 +57,9 @@ def lib():
         L.adgpu_ref_gen_and_eval_newpops.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp, vp]
         for n in ("perform_ls", "gradient_minad", "gradient_minadam"):
             getattr(L, f"adgpu_ref_{n}").argtypes = [C.c_uint32, C.c_uint32, vp, vp]
+        L.adgpu_ref_fire.argtypes = [vp, C.c_uint32, C.c_uint32, vp, vp]
+        L.adgpu_ref_get_gpudata.argtypes = [vp]
+        L.adgpu_ref_ocl_score.argtypes = [vp, C.c_uint32, vp, vp, vp]
         L.adgpu_ref_autostop_new.restype = vp
         L.adgpu_ref_autostop_new.argtypes = [C.c_int, C.c_int, C.c_float, C.c_int]
         L.adgpu_ref_autostop_check.restype = C.c_int
@@ -173,9 +176,32 @@ class RefJob:
         return (e, gr) if gradients else e
 
 
+def ocl_score(genotypes: np.ndarray):
+    """Energies and gene gradients from the reference's OpenCL merged scorer
+    (device/calcMergedEneGra.cl) for the bound job."""
+    L = lib()
+    g = np.ascontiguousarray(genotypes, np.float32)
+    n = g.shape[0]
+    e = np.zeros(n, np.float32)
+    gr = np.zeros((n, GENOTYPE_STRIDE), np.float32)
+    gd = C.create_string_buffer(L.adgpu_ref_sizeof_gpudata())
+    L.adgpu_ref_get_gpudata(C.cast(gd, C.c_void_p))
+    L.adgpu_ref_ocl_score(C.cast(gd, C.c_void_p), n, _ptr(g), _ptr(e), _ptr(gr))
+    return e, gr
+
+
 def call(name, *args):
     L = lib()
     conv = [(_ptr(a) if isinstance(a, np.ndarray) else a) for a in args]
+    if name in ("gradient_minfire", "gradient_minfire_asis"):
+        # the OpenCL FIRE kernel (device/kernel_fire.cl) takes its tables as
+        # arguments: hand it the bound job's GpuData.  "_asis" keeps the
+        # kernel's own first gradient, computed on coordinates it never
+        # initialises (ref/ref_fire_tu.cpp)
+        C.c_int.in_dll(L, "adgpu_ref_fire_first_gradient").value = 0 if name.endswith("_asis") else 1
+        gd = C.create_string_buffer(L.adgpu_ref_sizeof_gpudata())
+        L.adgpu_ref_get_gpudata(C.cast(gd, C.c_void_p))
+        return L.adgpu_ref_fire(C.cast(gd, C.c_void_p), *conv)
     return getattr(L, f"adgpu_ref_{name}")(*conv)
 
 

@@ -9,7 +9,8 @@ engine can be checked against them anywhere.
 Each fixture holds the reference-prepared tables of a seeded synthetic case
 (the grid is regenerated from its seed by adgpu_b200.synth), seeded
 genotypes with the reference scorer's energies and gradients, one GA
-generation and short local searches with the PRNG states before and after.
+generation and short local searches (Solis-Wets, ADADELTA, ADAM from its CUDA
+kernels, FIRE from its OpenCL kernel) with the PRNG states before and after.
 """
 import os
 import sys
@@ -108,7 +109,10 @@ def make(name, kw, tmp):
     # short local searches (4 iterations) from the GA offspring
     dp = abi.Dockpars.from_bytes(bytes(case.dockpars))
     dp.max_num_of_iters = 4
-    for meth in ("perform_ls", "gradient_minad", "gradient_minadam"):
+    # FIRE: the reference's OpenCL kernel (device/kernel_fire.cl) with its first
+    # gradient from its merged scorer (its own first call reads coordinates it
+    # never initialises, oracle/ref/ref_fire_tu.cpp)
+    for meth in ("perform_ls", "gradient_minad", "gradient_minadam", "gradient_minfire"):
         pr2 = out["ga_prng_after"].copy()
         en2 = np.zeros(R * P, np.int32)
         job.bind(pr2, en2, er.copy(), dockpars=bytes(dp))

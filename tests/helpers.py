@@ -82,6 +82,39 @@ def in_box_genotypes(case: Case, n: int, seed: int = 0, spread: float = 2.5) -> 
     return g
 
 
+def uniform_box_genotypes(case: Case, n: int, seed: int = 0) -> np.ndarray:
+    """The plain configuration's scorer sample: translations uniform over the
+    grid box (grid units), orientations uniform on SO(3) (Shoemake, as
+    gen_initpop_and_reflig draws them), torsions uniform in [-180, 180)."""
+    g = in_box_genotypes(case, n, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    gs = np.array(list(case.info.gridsize), np.float64)
+    g[:, :3] = rng.uniform(0.0, 1.0, (n, 3)) * (gs - 1.0)[None, :]
+    g[:, 6:case.ngenes] = rng.uniform(-180.0, 180.0, (n, case.ngenes - 6))
+    return g
+
+
+def energy_contract(ref: np.ndarray, terms: np.ndarray) -> np.ndarray:
+    """The energy rule for identical genotypes: |dE| <= 1e-4 |E| + 1e-6 * sum of
+    |terms| (the seven energy terms and the out-of-grid penalties, 2^24 per
+    atom outside), the floor covering cancellation between large terms."""
+    mag = np.abs(terms[:, :7]).sum(axis=1) + 16777216.0 * terms[:, 7]
+    return 1e-4 * np.abs(ref) + 1e-6 * mag
+
+
+def gradient_contract(case: Case, ref: np.ndarray) -> np.ndarray:
+    """The gradient rule for identical genotypes: |dg| <= 1e-4 |g| + n_terms /
+    1024 in gene units, n_terms the quantised terms that feed a gene (every
+    atom's intermolecular term and both ends of every intramolecular pair),
+    genes >= 3 scaled by spacing^2 / DEG_TO_RAD^2."""
+    ng = case.ngenes
+    n_terms = case.info.num_of_atoms + 2 * case.info.num_of_intraE_contributors
+    sp = case.info.spacing
+    scale = np.ones(ng, np.float64)
+    scale[3:] = sp * sp / (0.0174533 ** 2)
+    return 1e-4 * np.abs(ref[..., :ng]) + scale * n_terms / 1024.0
+
+
 def energy_tolerance(ref: np.ndarray) -> np.ndarray:
     """|dE| <= 1e-4 |E| + 1e-6 * |E| floor -> effectively 1e-4 relative with a 1e-3 absolute floor."""
     return 1e-4 * np.abs(ref) + 1e-3

@@ -82,8 +82,11 @@ def test_ga_generation(case, tpp, monkeypatch):
     ("fire", "adgpu_gradient_minfire", "gradient_minfire"),
 ])
 @pytest.mark.parametrize("iters", [5, 300])
-def test_local_search(case, method, entry, oracle_fn, iters, monkeypatch):
-    dj, host, st, dp = _setup(case, max_iters=iters, monkeypatch=monkeypatch)
+@pytest.mark.parametrize("tpp", [32, 64])
+def test_local_search(case, method, entry, oracle_fn, iters, tpp, monkeypatch):
+    """32 threads per pose: the pipelined docking loop's group size; 64: the
+    per-generation launches' for Solis-Wets and ADADELTA."""
+    dj, host, st, dp = _setup(case, max_iters=iters, tpp=tpp, monkeypatch=monkeypatch)
     R, P = case.runs, dp.pop_size
     L = dp.num_of_lsentities
     cur, ecur = dj.population(case.initpop)

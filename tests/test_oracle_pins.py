@@ -103,3 +103,77 @@ def test_sum_evals_and_initpop(case):
     case.host.call("sum_evals", R)
     assert np.all(np.abs(e1 - e2) <= 1e-5 * np.abs(e1) + 1e-4)
     assert np.array_equal(err, ero) and err.tolist() == [P] * R
+
+
+@pytest.mark.parametrize("iters,min_close", [(1, 1.0), (4, 0.95)])
+def test_fire_matches_reference_opencl_source(case, iters, min_close):
+    """The oracle's FIRE against the reference's OpenCL FIRE kernel
+    (device/kernel_fire.cl under the emulator), the reference's first
+    gradient taken from its merged scorer: the same PRNG draws and evaluation
+    counts, and genotypes that agree entity by entity (one step: all within
+    1e-2; four steps: rounding can flip a step-size decision)."""
+    dp = case.dockpars.copy()
+    dp.max_num_of_iters = iters
+    R, P = case.runs, dp.pop_size
+    nb = min(R * dp.num_of_lsentities, 60)
+    pr, po, enr, eno, err, ero = _bind(case, dp)
+    pop = case.initpop[:R * P].copy()
+    e = case.host.score(pop, False)
+    a_c, a_e, b_c, b_e = pop.copy(), e.copy(), pop.copy(), e.copy()
+    refpy.call("gradient_minfire", nb, T, a_c, a_e)
+    case.host.call("gradient_minfire", nb, T, b_c, b_e, 2)
+    assert np.array_equal(pr, po)
+    assert np.array_equal(enr, eno)
+    ng = case.ngenes
+    close = np.abs(a_c[:nb, :ng] - b_c[:nb, :ng]).max(axis=1) <= 1e-2
+    assert close.mean() >= min_close
+    assert np.all(np.abs(a_e[:nb] - b_e[:nb]) <= 1e-3 * np.abs(a_e[:nb]) + 1e-2) or iters > 1
+
+
+def test_reference_fire_first_gradient_reads_uninitialised_coordinates(case):
+    """Why the engine takes FIRE's first gradient from the merged scorer: the
+    reference's own first call (gpu_calc_gradient, kernel_fire.cl:318)
+    rotates the kernel's __local calc_coords without loading the reference
+    coordinates into them (calcgradient.cl:160-258), so its first step does
+    not follow the entity's gradient: after one step its genotypes are far
+    from those of a step along the merged scorer's gradient, which the oracle
+    reproduces to rounding."""
+    dp = case.dockpars.copy()
+    dp.max_num_of_iters = 1
+    R, P = case.runs, dp.pop_size
+    nb = min(R * dp.num_of_lsentities, 60)
+    pop = case.initpop[:R * P].copy()
+    e = case.host.score(pop, False)
+    out = {}
+    for name in ("gradient_minfire_asis", "gradient_minfire"):
+        _bind(case, dp)
+        c, ee = pop.copy(), e.copy()
+        refpy.call(name, nb, T, c, ee)
+        out[name] = c[:nb, :case.ngenes]
+    _bind(case, dp)
+    c, ee = pop.copy(), e.copy()
+    case.host.call("gradient_minfire", nb, T, c, ee, 2)
+    ng = case.ngenes
+    d_oracle = np.abs(c[:nb, :ng] - out["gradient_minfire"]).max(axis=1)
+    d_asis = np.abs(out["gradient_minfire_asis"] - out["gradient_minfire"]).max(axis=1)
+    assert np.median(d_oracle) < 1e-2
+    assert np.median(d_asis) > 10 * max(np.median(d_oracle), 1e-3)
+
+
+def test_reference_opencl_scorer_translation_gradient(case, flex_case):
+    """The reference's two merged scorers agree on a rigid receptor, and with
+    flexible residues its OpenCL one (used by its FIRE) sums the translation
+    gradient over the residues' atoms as well (calcMergedEneGra.cl:635-649;
+    the CUDA one, calcMergeEneGra.cu:616-640, over the ligand's atoms only):
+    the oracle and the engine follow the CUDA scorer for every search."""
+    for c, flex in ((case, False), (flex_case, True)):
+        _bind(c)
+        g = helpers.in_box_genotypes(c, 32, seed=11)
+        e_cu, g_cu = c.job.score(g, True)
+        e_cl, g_cl = refpy.ocl_score(g)
+        assert np.all(np.abs(e_cu - e_cl) <= 1e-5 * np.abs(e_cu) + 1e-4)
+        d = np.abs(g_cu[:, :3] - g_cl[:, :3])
+        if flex:
+            assert np.median(d) > 0.1
+        else:
+            assert d.max() <= 4.0 / 1024.0 + 1e-4 * np.abs(g_cu[:, :3]).max()

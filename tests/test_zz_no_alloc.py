@@ -1,8 +1,8 @@
 """adgpu_score_genotypes_noalloc: the scorer variant that allocates no device
-memory.  Through the C ABI it must score as adgpu_score_genotypes does, on
-two calls in a row and after another ligand has used its fixed scratch
-array, and reject ligands beyond that array's size before touching the
-device.  The file is named to collect last, so it also runs after the rest
+memory.  Through the C ABI it must score as adgpu_score_genotypes does and
+as the oracle does, on two calls in a row and after another ligand has used
+its fixed scratch array, and reject ligands beyond that array's size before
+touching the device.  The file is named to collect last, so it also runs after the rest
 of the GPU suite in one process."""
 import ctypes as C
 
@@ -57,6 +57,13 @@ def test_noalloc_matches_scorer_on_consecutive_calls(cases):
             assert np.all(diff <= helpers.gradient_bound(case, gr_ref)), diff.max(axis=0)
         assert np.array_equal(first[0], second[0]) and np.array_equal(first[1][:, :ng], second[1][:, :ng])
         assert np.all(np.abs(e_only - e_ref_only) <= helpers.energy_tolerance(e_ref_only))
+        # and against the oracle directly (its own code path reads the
+        # caller's reference-layout grid, which no other entry point does)
+        e_or, gr_or = case.host.score(gh, True, nthreads=8)
+        terms = np.array([case.host.score_terms(x)[2] for x in gh])
+        assert np.all(np.abs(first[0] - e_or) <= helpers.energy_contract(e_or, terms)), np.abs(first[0] - e_or).max()
+        d = np.abs(first[1][:, :ng] - gr_or[:, :ng])
+        assert np.all(d <= helpers.gradient_bound(case, gr_or)), d.max(axis=0)
 
 
 @pytest.mark.gpu
@@ -89,3 +96,30 @@ def test_noalloc_rejects_ligands_beyond_its_scratch():
     assert "1048576" in L.adgpu_last_error().decode()
     st = L.adgpu_score_genotypes_noalloc(None, 10, buf, buf, buf)
     assert st == 1, st
+    # more map types than the reference's limit (the cell-record slot of an
+    # atom is 8 bits wide)
+    dp.num_of_intraE_contributors = 100
+    dp.num_of_map_atypes = 40
+    st = L.adgpu_score_genotypes_noalloc(C.cast(C.pointer(g), C.c_void_p), 10, buf, buf, buf)
+    assert st == 4, (st, L.adgpu_last_error())
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_a_rotation_list_naming_no_atom(cases):
+    """A rotation-list entry whose atom index is past the ligand's atoms is an
+    error (the device repack checks every entry; no access depends on it)."""
+    from adgpu_b200 import device
+    case = cases["cfg2"]
+    tables = dict(case.tables)
+    rl = np.frombuffer(bytes(tables["rotlist"]), np.int32).copy()
+    N = case.dockpars.num_of_atoms
+    k = int(np.nonzero((rl[:case.dockpars.rotbondlist_length] & abi.RLIST_DUMMY_MASK) == 0)[0][0])
+    rl[k] = (rl[k] & ~abi.RLIST_ATOMID_MASK) | N
+    tables["rotlist"] = rl.view(np.uint8)
+    job = device.DeviceJob(tables, case.dockpars, case.grid, case.runs, case.prng)
+    g = torch.from_numpy(helpers.in_box_genotypes(case, 8, seed=1)).cuda()
+    e = torch.zeros(8, dtype=torch.float32, device="cuda")
+    st = lib.load().adgpu_score_genotypes_noalloc(C.cast(C.pointer(job.g), C.c_void_p), 8, C.c_void_p(g.data_ptr()),
+                                                  C.c_void_p(e.data_ptr()), None)
+    assert st == 1, st
+    assert b"out of range" in lib.load().adgpu_last_error()
