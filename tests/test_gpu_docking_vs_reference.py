@@ -115,3 +115,54 @@ def test_docking_matches_reference_cuda_statistically(tmp_path, lsmet, size):
     assert abs(egen - rgen) <= max(3, 0.1 * rgen)          # the same evaluation budget spent alike
     assert ks.pvalue > 1e-3, ks
     assert e_in_r < 2.0 and r_in_e < 2.0, (e_in_r, r_in_e)
+
+
+def oracle_docking(case, lsmet, nev, nthreads=8):
+    """docking_with_gpu's loop over the oracle's kernels on the host (the
+    oracle's FIRE is pinned to the reference's OpenCL kernel,
+    tests/test_oracle_pins.py; the reference has no CUDA FIRE to run)."""
+    dp = case.dockpars
+    R, P, L = case.runs, dp.pop_size, dp.num_of_lsentities
+    ht = case.host
+    ht.g.dockpars = dp
+    prng = case.prng.copy()
+    en, er = np.zeros(R * P, np.int32), np.zeros(R, np.int32)
+    ht.bind_state(prng, en, er)
+    cur = case.initpop[:R * P].copy()
+    ecur = np.zeros(R * P, np.float32)
+    nxt, enxt = np.zeros_like(cur), np.zeros_like(ecur)
+    ht.call("calc_initpop", R * P, cur, ecur, nthreads)
+    ht.call("sum_evals", R)
+    gens = 0
+    while er.sum() / R < nev:
+        ht.call("gen_and_eval_newpops", R * P, T, cur, ecur, nxt, enxt, nthreads)
+        ht.call(f"gradient_min{lsmet}", R * L, T, nxt, enxt, nthreads)
+        ht.call("sum_evals", R)
+        gens += 1
+        cur, nxt, ecur, enxt = nxt, cur, enxt, ecur
+    return torch.from_numpy(cur), torch.from_numpy(ecur), gens
+
+
+def test_fire_docking_matches_oracle_statistically(tmp_path):
+    """FIRE whole dockings (cfg1 ligand, 32 runs of 2.5M evaluations) against
+    the oracle's, which follows the reference's OpenCL FIRE: same generation
+    count, run best energies from the same distribution, top binding modes
+    within 2 A of each other's three best clusters."""
+    from scipy import stats
+    case = helpers.make_case(str(tmp_path), 40, ["C", "A", "N", "OA", "HD"], 16, 4, 32, config_id=1, lsmet="fire")
+    nev = 2_500_000
+    rc, re_, rgen = oracle_docking(case, "fire", nev)
+    ec, ee, egen, _ = engine_docking(case, "fire", nev)
+    r_tops, r_scorer = top_clusters(case, rc, re_)
+    e_tops, e_scorer = top_clusters(case, ec, ee)
+    ks = stats.ks_2samp(e_scorer, r_scorer)
+    N = case.info.true_ligand_atoms
+    types = case.tables["interintra"][1024:2048].view(np.uint32)[:N]
+    e_in_r = min(sym_rmsd(e_tops[0][0][:N], t[0][:N], types) for t in r_tops)
+    r_in_e = min(sym_rmsd(r_tops[0][0][:N], t[0][:N], types) for t in e_tops)
+    print(json.dumps({"lsmet": "fire", "generations": [egen, rgen], "ks_p": float(ks.pvalue),
+                      "best_energy_median": [float(np.median(e_scorer)), float(np.median(r_scorer))],
+                      "top": [e_in_r, r_in_e]}))
+    assert abs(egen - rgen) <= max(3, 0.1 * rgen)
+    assert ks.pvalue > 1e-3, ks
+    assert e_in_r < 2.0 and r_in_e < 2.0
