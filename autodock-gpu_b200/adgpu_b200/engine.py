@@ -14,7 +14,8 @@ LSMET = {"sw": 0, "ad": 1, "adam": 2, "fire": 3}
 
 class EngineConfig(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_size_t), ("threads_per_pose", C.c_int),
-                ("gens_per_tick", C.c_int), ("device", C.c_int), ("tick_ms", C.c_float)]
+                ("gens_per_tick", C.c_int), ("device", C.c_int), ("tick_ms", C.c_float),
+                ("idle_timeout_ms", C.c_float)]
 
 
 class RequestParams(C.Structure):
@@ -22,7 +23,7 @@ class RequestParams(C.Structure):
 
 
 class EngineStats(C.Structure):
-    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("ticks", C.c_uint64),
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("cancelled", C.c_uint64), ("ticks", C.c_uint64),
                 ("bytes_used", C.c_size_t), ("bytes_budget", C.c_size_t), ("active", C.c_int),
                 ("worker_busy_s", C.c_double), ("worker_span_s", C.c_double), ("tasks", C.c_uint64),
                 ("kernel_s", C.c_double)]
@@ -39,6 +40,8 @@ SIGNATURES = {
     "adgpu_engine_poll": (C.c_int, [_vp, C.c_uint64, _vp]),
     "adgpu_engine_result": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp, _vp, _vp]),
     "adgpu_engine_stats_get": (C.c_int, [_vp, _vp]),
+    "adgpu_engine_cancel": (C.c_int, [_vp, C.c_uint64]),
+    "adgpu_engine_inject_stall": (C.c_int, [_vp, C.c_uint64]),
     "adgpu_engine_request_info": (C.c_int, [_vp, C.c_uint64, _vp, _vp]),
     "adgpu_engine_process_result": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
@@ -69,8 +72,8 @@ class Result:
 
 class Engine:
     def __init__(self, memory_budget_bytes: int = 0, threads_per_pose: int = 0, gens_per_tick: int = 0,
-                 device: int = 0, tick_ms: float = 0.0):
-        cfg = EngineConfig(memory_budget_bytes, threads_per_pose, gens_per_tick, device, tick_ms)
+                 device: int = 0, tick_ms: float = 0.0, idle_timeout_ms: float = 0.0):
+        cfg = EngineConfig(memory_budget_bytes, threads_per_pose, gens_per_tick, device, tick_ms, idle_timeout_ms)
         h = C.c_void_p()
         lib.check(_L().adgpu_engine_create(C.byref(cfg), C.byref(h)), "engine_create")
         self.h = h
@@ -112,6 +115,16 @@ class Engine:
 
     def run(self):
         lib.check(_L().adgpu_engine_run(self.h), "engine_run")
+
+    def cancel(self, request_id: int):
+        """Drops a request (finished or not) between ticks."""
+        lib.check(_L().adgpu_engine_cancel(self.h, request_id), "engine_cancel")
+        self._pop_size.pop(request_id, None)
+
+    def inject_stall(self, request_id: int):
+        """Test hook: the request's runs stop handing out tasks (the next tick
+        times out after idle_timeout_ms)."""
+        lib.check(_L().adgpu_engine_inject_stall(self.h, request_id), "engine_inject_stall")
 
     def done(self, request_id: int) -> bool:
         d = C.c_int()

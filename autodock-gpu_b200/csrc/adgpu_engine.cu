@@ -42,6 +42,7 @@ struct ReqDev {
 	float* e[2];                // R*P
 	int* evals_runs;            // R
 	int* pending;               // R tasks of the run's current phase not yet done
+	unsigned long long* next;   // R the run's open phase << 32 | entities handed out
 	uint32_t* gen;              // R generations done
 	uint8_t* cur;               // R current buffer index
 	uint8_t* done;              // R run finished
@@ -64,29 +65,32 @@ constexpr int kEngineThreads = 128;
 #endif
 
 // --------------------------------------------------------------------------
-// task queue
+// scheduling
 // --------------------------------------------------------------------------
-// A run advances through phases -- initial population, GA generation, local
-// search -- and each phase is split into independent tasks: a chunk of GA
-// (or initial-population) entities, or one local-search entity.  Tasks of a
-// class (threads per pose) go through one FIFO ring; the pose group that
-// completes the last task of a phase finalises it (eval sum, stop test) and
-// pushes the run's next tasks.  A generation's local searches therefore run
-// on as many pose groups as the run has local-search entities, and no group
-// waits for another run's slowest entity.
-enum : uint32_t { kTaskStart = 0, kTaskInit = 1, kTaskGA = 2, kTaskLS = 3 };
-constexpr uint32_t kTaskIdxBits = 11;                          // entity / chunk index < 2048
-constexpr uint32_t kMaxTickRuns = 1u << (32 - kTaskIdxBits - 2); // run index bits
-constexpr int kSlotSpin = 1 << 20;                             // polls of a reserved slot's write
-constexpr long long kIdleNs = 20000000;                        // an idle worker retires after 20 ms
+// A run advances in steps: step 0 scores its initial population, step s >= 1
+// is generation s-1.  Each step is split into one task per entity.  For a
+// generation a task is the GA step that makes the entity (elitism, or
+// tournaments, crossover, mutation and scoring) followed, at the reference's
+// default 100 % local-search rate, by the entity's local search, both on the
+// entity's own PRNG states in the reference's order; at a lower rate the
+// local searches form a second phase of their own (the entity a search takes
+// may be one another task makes).  A run hands out the entities of its
+// current phase from one counter (phase << 32 | entities taken; phase =
+// 2*step, or 2*step+1 for a separate local-search phase), kept per work item
+// for the tick.  A pose group keeps taking entities of the run it served
+// last and otherwise scans its class's runs for the least advanced one with
+// entities left; the group that completes a phase's last task finalises it
+// (eval sum, stop test) and opens the run's next phase.  No run waits for
+// another, and no run's generation waits behind another run's.
+struct TickRun {
+	unsigned long long next;    // phase << 32 | entities taken
+	int ntasks;                 // entities of the open phase (a hint for the scan)
+	int limit;                  // steps at or above this one do not start in this tick
+};
 
-__host__ __device__ constexpr uint32_t task_word(uint32_t w, uint32_t kind, uint32_t idx)
-{
-	return (w << (kTaskIdxBits + 2)) | (kind << kTaskIdxBits) | idx;
-}
-
-// A class's ring (adgpu_queue.cuh) and the CTAs that serve it.
-struct TickClass : TaskRing {
+struct TickClass {
+	QueueCtl* ctl;              // alive (runs not finished or parked this tick), err, accounting
+	int w0, nw;                 // this class's work items
 	int cta_end;                // this class's CTAs are [previous class's cta_end, cta_end)
 	int group_bytes;            // shared memory per pose group
 };
@@ -94,25 +98,112 @@ struct TickClass : TaskRing {
 struct TickArgs {
 	const ReqDev* reqs;
 	const RunRef* work;
+	TickRun* runs;              // per work item
 	uint8_t* work_done;         // per work item: run finished (written when it retires)
-	int* quota;                 // per work item: phases this tick may still run
-	int ga_chunk;               // entities per GA / initial-population task
 	long long tick_ns;          // > 0: a worker takes no new task once this long after it started
+	long long idle_ns;          // a worker that finds no task for this long stops and reports an error
 	TickClass cls[3];           // threads per pose 32, 64, 128
 };
 
+constexpr int kScanWindow = 4096;                              // work items one scan looks at
+constexpr long long kIdleNs = 2000000000ll;                    // default idle limit (2 s)
+
 // Per-pose-group header in shared memory, ahead of the group's scratch.
 struct GroupHdr {
-	KArgs a;                    // the current request's arguments, pointers set per task
-	unsigned long long pos;
+	KArgs a;                    // the current request's arguments
 	long long t_enter, t_task;           // worker accounting (rank 0 only)
 	long long deadline;                  // globaltimer after which no task is taken; 0: none
 	unsigned long long busy, ntask;
-	int task, last, req, next, cur, isum;
+	int task_w, task_idx, req, last, next, cur, isum, sticky;
+	unsigned int task_phase;
 	float bv[4];
 	int bi[4];
 };
 constexpr int kHdrBytes = (int)((sizeof(GroupHdr) + 15) / 16 * 16);
+
+__device__ __forceinline__ int phase_tasks(const ReqDev& rq, unsigned int phase)
+{
+	return (phase & 1u) ? (int)rq.a.dp.num_of_lsentities : rq.a.dp.pop_size;
+}
+
+// The next task for this pose group (called by its first warp): work item,
+// phase and entity in *w, *phase, *idx; false when the worker should stop
+// (deadline, nothing left in its class, or the idle limit: error).
+template <int TPP>
+__device__ bool take_task(const TickArgs& t, const TickClass& C, int lane, int worker, GroupHdr& H,
+                          int* w_out, unsigned int* phase_out, int* idx_out)
+{
+	volatile QueueCtl* vq = C.ctl;
+	long long idle_since = -1;
+	int backoff = 64;
+	unsigned int rot = (unsigned int)worker * 2654435761u;
+	for (int spins = 0; spins < (1 << 30); spins++) {
+		if (H.deadline && global_ns() > H.deadline) return false;
+		// the run served last, then a scan for the least advanced run with entities left
+		int cand = -1;
+		if (spins == 0 && H.sticky >= 0) {
+			cand = H.sticky;
+		} else {
+			unsigned long long best = ~0ull;
+			const int n = C.nw < kScanWindow ? C.nw : kScanWindow;
+			const int off = C.nw <= kScanWindow ? 0 : (int)((rot + (unsigned)spins * 977u) % (unsigned)C.nw);
+			for (int i = lane; i < n; i += 32) {
+				int w = off + i;
+				if (w >= C.nw) w -= C.nw;
+				w += C.w0;
+				const int4 r = __ldcv(reinterpret_cast<const int4*>(t.runs + w));
+				const unsigned int taken = (unsigned int)r.x, phase = (unsigned int)r.y;
+				const int step = (int)(phase >> 1);
+				if (taken < (unsigned int)r.z && step < r.w) {
+					const unsigned long long key = ((unsigned long long)(unsigned int)step << 32) |
+					                               (((unsigned int)w - (unsigned int)C.w0 + rot) % (unsigned int)C.nw);
+					best = key < best ? key : best;
+				}
+			}
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) {
+				const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
+				best = x < best ? x : best;
+			}
+			if (best != ~0ull) cand = C.w0 + (int)(((unsigned int)best - rot % (unsigned int)C.nw + (unsigned int)C.nw) %
+			                                       (unsigned int)C.nw);
+		}
+		if (cand >= 0) {
+			unsigned long long old = 0;
+			int ok = 0;
+			if (lane == 0) {
+				const int4 r = __ldcv(reinterpret_cast<const int4*>(t.runs + cand));
+				if ((unsigned int)r.x < (unsigned int)r.z && (int)((unsigned int)r.y >> 1) < r.w) {
+					old = atomicAdd(&t.runs[cand].next, 1ull);
+					const unsigned int phase = (unsigned int)(old >> 32), idx = (unsigned int)old;
+					const ReqDev& rq = t.reqs[t.work[cand].req];
+					ok = idx < (unsigned int)phase_tasks(rq, phase) && (int)(phase >> 1) < t.runs[cand].limit;
+				}
+			}
+			ok = __shfl_sync(0xffffffffu, ok, 0);
+			old = __shfl_sync(0xffffffffu, old, 0);
+			if (ok) {
+				__threadfence();
+				*w_out = cand;
+				*phase_out = (unsigned int)(old >> 32);
+				*idx_out = (int)(unsigned int)old;
+				return true;
+			}
+			if (spins == 0) continue;      // the sticky run had nothing left: scan at once
+		}
+		if (vq->alive <= 0) return false;
+		const long long now = global_ns();
+		if (idle_since < 0) idle_since = now;
+		else if (now - idle_since > t.idle_ns) {
+			if (lane == 0) atomicExch(&C.ctl->err, 1);
+			return false;
+		}
+		__nanosleep(backoff);
+		if (backoff < 4096) backoff *= 2;
+	}
+	if (lane == 0) atomicExch(&C.ctl->err, 2);
+	return false;
+}
 
 template <int TPP>
 __device__ int group_isum(int v, const Group<TPP>& G, GroupHdr& H)
@@ -160,7 +251,17 @@ __device__ void best_of_run(const ReqDev& rq, int run, int c, int P, const Group
 	G.sync();
 }
 
-enum : int { kNextRetire = 0, kNextBest = 1, kNextInit = 2, kNextGA = 3 };
+// Opens phase `phase` of work item w (its run's counter and the tick's
+// copy), or parks the run when the phase's step is past the tick's limit.
+__device__ void open_phase(const TickArgs& t, const TickClass& C, const ReqDev& rq, int w, int run, unsigned int phase)
+{
+	const int n = phase_tasks(rq, phase);
+	rq.pending[run] = n;
+	t.runs[w].ntasks = n;
+	__threadfence();
+	atomicExch(&t.runs[w].next, (unsigned long long)phase << 32);
+	if ((int)(phase >> 1) >= t.runs[w].limit) atomicSub(&C.ctl->alive, 1);      // parked until the next tick
+}
 
 template <int TPP, int LSMET>
 __device__ void engine_worker(const TickArgs& t, const TickClass& C)
@@ -174,25 +275,33 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 	G.rank = threadIdx.x % TPP;
 	G.bar_id = 1 + local;
 	G.red = nullptr;
+	const int worker = blockIdx.x * (kEngineThreads / TPP) + local;
 	if (G.rank == 0) {
-		H.req = -1; H.t_enter = global_ns(); H.t_task = 0; H.busy = 0; H.ntask = 0;
+		H.req = -1; H.sticky = -1; H.t_enter = global_ns(); H.t_task = 0; H.busy = 0; H.ntask = 0;
 		H.deadline = t.tick_ns > 0 ? H.t_enter + t.tick_ns : 0;
 	}
 	G.sync();
 	for (;;) {
-		if (G.rank == 0) {
-			if (H.t_task) H.busy += (unsigned long long)(global_ns() - H.t_task);
-			H.task = ring_pop(C, H.deadline);
-			H.t_task = H.task >= 0 ? global_ns() : 0;
-			H.ntask += H.task >= 0;
+		if (G.rank < 32) {
+			if (G.rank == 0 && H.t_task) H.busy += (unsigned long long)(global_ns() - H.t_task);
+			int w = -1, idx = 0;
+			unsigned int phase = 0;
+			const bool got = take_task<TPP>(t, C, G.rank, worker, H, &w, &phase, &idx);
+			if (G.rank == 0) {
+				H.task_w = got ? w : -1;
+				H.task_phase = phase;
+				H.task_idx = idx;
+				H.t_task = got ? global_ns() : 0;
+				H.ntask += got;
+				if (got) H.sticky = w;
+			}
 		}
 		G.sync();
-		const int task = H.task;
-		if (task < 0) break;
+		const int w = H.task_w;
+		if (w < 0) break;
 		__threadfence();
-		const uint32_t w = (uint32_t)task >> (kTaskIdxBits + 2);
-		const uint32_t kind = ((uint32_t)task >> kTaskIdxBits) & 3u;
-		const int idx = task & (int)((1u << kTaskIdxBits) - 1);
+		const unsigned int phase = H.task_phase;
+		const int idx = H.task_idx;
 		const RunRef rr = t.work[w];
 		const ReqDev& rq = t.reqs[rr.req];
 		const int run = rr.run;
@@ -203,57 +312,55 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 			G.sync();
 			if (G.rank == 0) H.req = rr.req;
 		}
+		G.sync();
 		KArgs& a = H.a;
 		const GroupSmem S = carve_group(scratch, a.L.natoms, a.L.ntors, 64, TPP);
 		G.red = S.red;
 		const int P = a.dp.pop_size;
 		const int L = (int)a.dp.num_of_lsentities;
-		if (kind != kTaskStart) {
-			const int c = rq.cur[run];
-			if (G.rank == 0) {
-				if (kind == kTaskInit) { a.conf = rq.conf[c]; a.e = rq.e[c]; a.prng = rq.a.prng; }
-				else if (kind == kTaskGA) {
-					a.conf_cur = rq.conf[c]; a.e_cur = rq.e[c];
-					a.conf = rq.conf[c ^ 1]; a.e = rq.e[c ^ 1];
-					a.prng = rq.a.prng;
-				} else {
-					// local search on the next population; entity l of run r uses
-					// the PRNG states of GA block r*P + l (its own run's range), so
-					// runs in different phases never share states
-					a.conf = rq.conf[c ^ 1]; a.e = rq.e[c ^ 1];
-					a.prng = rq.a.prng + (size_t)run * (size_t)(P - L) * 64;
+		const bool fused = L == P;
+		const int c = rq.cur[run];
+		if (phase == 0) {
+			// step 0: the initial population's energies (cuda/kernel1.cu:26-55)
+			initpop_block<TPP>(a, PopBufs{nullptr, nullptr, rq.conf[c], rq.e[c]}, (uint32_t)(run * P + idx), G, S);
+		} else {
+			const bool ls_phase = (phase & 1u) != 0;
+			if (!ls_phase) ga_block<TPP>(a, PopBufs{rq.conf[c], rq.e[c], rq.conf[c ^ 1], rq.e[c ^ 1]},
+			                             (uint32_t)(run * P + idx), G, S);
+			if (ls_phase || (fused && L > 0)) {
+				// local-search block run*L + idx; entity l of run r draws from
+				// the PRNG states of GA block r*P + l (its own run's range: the
+				// offset is zero when every entity is searched)
+				if (ls_phase) {
+					if (G.rank == 0) a.prng = rq.a.prng + (size_t)run * (size_t)(P - L) * 64;
+					G.sync();
 				}
-			}
-			G.sync();
-			if (kind == kTaskLS) {
+				const PopBufs pb{nullptr, nullptr, rq.conf[c ^ 1], rq.e[c ^ 1]};
 				const uint32_t b = (uint32_t)(run * L + idx);
-				if constexpr (LSMET == LS_SW) sw_block<TPP>(a, b, G, S);
-				else if constexpr (LSMET == LS_AD) gradient_ls_block<TPP, LS_AD>(a, b, G, S);
-				else if constexpr (LSMET == LS_ADAM) gradient_ls_block<TPP, LS_ADAM>(a, b, G, S);
-				else fire_block<TPP>(a, b, G, S);
-			} else {
-				const int e0 = idx * t.ga_chunk, e1 = min(P, e0 + t.ga_chunk);
-				for (int e = e0; e < e1; e++) {
-					if (kind == kTaskInit) initpop_block<TPP>(a, (uint32_t)(run * P + e), G, S);
-					else ga_block<TPP>(a, (uint32_t)(run * P + e), G, S);
+				if constexpr (LSMET == LS_SW) sw_block<TPP>(a, pb, b, G, S);
+				else if constexpr (LSMET == LS_AD) gradient_ls_block<TPP, LS_AD>(a, pb, b, G, S);
+				else if constexpr (LSMET == LS_ADAM) gradient_ls_block<TPP, LS_ADAM>(a, pb, b, G, S);
+				else fire_block<TPP>(a, pb, b, G, S);
+				if (ls_phase) {
+					if (G.rank == 0) a.prng = rq.a.prng;
+					G.sync();
 				}
 			}
-			// the last task of the phase goes on to finalise it
-			__threadfence();
-			G.sync();
-			if (G.rank == 0) H.last = (atomicSub(&rq.pending[run], 1) == 1);
-			G.sync();
-			if (!H.last) continue;
-			__threadfence();
 		}
+		// the last task of the phase goes on to finalise it
+		__threadfence();
+		G.sync();
+		if (G.rank == 0) H.last = (atomicSub(&rq.pending[run], 1) == 1);
+		G.sync();
+		if (!H.last) continue;
+		__threadfence();
 		// ---- phase end ----
-		if (kind == kTaskGA && L > 0 && a.dp.lsearch_rate != 0.0f) {
-			if (G.rank == 0) { rq.pending[run] = L; __threadfence(); }
+		if (phase != 0 && (phase & 1u) == 0 && !fused && L > 0) {
+			if (G.rank == 0) open_phase(t, C, rq, w, run, phase + 1);
 			G.sync();
-			ring_push(C, task_word(w, kTaskLS, 0), L, G, H.pos);
 			continue;
 		}
-		if (kind == kTaskGA || kind == kTaskLS) {
+		if (phase != 0) {
 			// eval sum of the run (cuda/kernel2.cu:26-52), generation count, buffer flip
 			int s = 0;
 			for (int i = G.rank; i < P; i += TPP) s += a.evals_new[run * P + i];
@@ -262,40 +369,29 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 				rq.evals_runs[run] += s;
 				rq.gen[run] += 1;
 				rq.cur[run] = (uint8_t)(rq.cur[run] ^ 1);
-				t.quota[w] -= 1;
 			}
-		} else if (kind == kTaskInit) {
-			if (G.rank == 0) { rq.init[run] = 1; rq.evals_runs[run] = P; t.quota[w] -= 1; }
+		} else if (G.rank == 0) {
+			rq.init[run] = 1;
+			rq.evals_runs[run] = P;
 		}
 		// stop test (per run: its own evaluations, or its generations)
 		if (G.rank == 0) {
-			int d = rq.done[run], next;
-			if (d) next = kNextRetire;
-			else if (rq.init[run] && ((unsigned long long)rq.evals_runs[run] >= rq.max_evals || rq.gen[run] >= rq.max_gens)) {
-				rq.done[run] = 1;
-				next = kNextBest;
-			} else if (t.quota[w] <= 0 || (H.deadline && global_ns() > H.deadline))
-				next = kNextRetire;
-			else next = rq.init[run] ? kNextGA : kNextInit;
-			H.next = next;
+			const bool stop = (unsigned long long)rq.evals_runs[run] >= rq.max_evals || rq.gen[run] >= rq.max_gens;
+			H.next = stop ? 1 : 0;
 			H.cur = rq.cur[run];
+			if (stop) rq.done[run] = 1;
+			else open_phase(t, C, rq, w, run, ((phase >> 1) + 1) << 1);
 		}
 		G.sync();
-		const int next = H.next;
-		if (next == kNextGA || next == kNextInit) {
-			const int nch = (P + t.ga_chunk - 1) / t.ga_chunk;
-			if (G.rank == 0) { rq.pending[run] = nch; __threadfence(); }
+		if (H.next) {
+			best_of_run<TPP>(rq, run, H.cur, P, G, H);
+			if (G.rank == 0) {
+				t.work_done[w] = 1;
+				__threadfence();
+				atomicSub(&C.ctl->alive, 1);
+			}
 			G.sync();
-			ring_push(C, task_word(w, next == kNextGA ? kTaskGA : kTaskInit, 0), nch, G, H.pos);
-			continue;
 		}
-		if (next == kNextBest) best_of_run<TPP>(rq, run, H.cur, P, G, H);
-		if (G.rank == 0) {
-			t.work_done[w] = rq.done[run];
-			__threadfence();
-			atomicSub(&C.ctl->alive, 1);
-		}
-		G.sync();
 	}
 	if (G.rank == 0) {
 		atomicAdd(&C.ctl->busy_ns, H.busy);
@@ -307,13 +403,49 @@ __device__ void engine_worker(const TickArgs& t, const TickClass& C)
 }
 
 // One kernel per local search; its CTAs are split into three ranges, one per
-// threads-per-pose class, each range serving its class's queue.
+// threads-per-pose class, each range serving its class's runs.
 template <int LSMET>
 __global__ void __launch_bounds__(kEngineThreads, ADGPU_ENGINE_MIN_CTAS) engine_kernel(const TickArgs t)
 {
 	if ((int)blockIdx.x < t.cls[0].cta_end) engine_worker<32, LSMET>(t, t.cls[0]);
 	else if ((int)blockIdx.x < t.cls[1].cta_end) engine_worker<64, LSMET>(t, t.cls[1]);
 	else engine_worker<128, LSMET>(t, t.cls[2]);
+}
+
+// Tick set-up and tear-down: each work item's phase counter from its run's
+// persistent state, with the tick's step limit, and back.  Runs that
+// finished in an earlier tick (their request is still waiting for others)
+// count as done at once; the rest are the classes' active runs.
+struct ClassBounds { int start[13]; };
+
+__global__ void __launch_bounds__(256) tick_load_kernel(const ReqDev* reqs, const RunRef* work, TickRun* runs,
+                                                         uint8_t* done, int n, int steps, QueueCtl* ctl, ClassBounds cb)
+{
+	for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < n; w += gridDim.x * blockDim.x) {
+		const ReqDev& rq = reqs[work[w].req];
+		const int run = work[w].run;
+		const unsigned long long v = rq.next[run];
+		const unsigned int phase = (unsigned int)(v >> 32);
+		const bool finished = rq.done[run] != 0;
+		TickRun r;
+		r.next = v;
+		r.ntasks = phase_tasks(rq, phase);
+		const long long lim = finished ? 0 : (long long)(phase >> 1) + steps;
+		r.limit = (int)(lim > 0x3fffffffll ? 0x3fffffffll : lim);
+		runs[w] = r;
+		done[w] = finished ? 1 : 0;
+		if (!finished) {
+			int c = 0;
+			while (c < 12 && w >= cb.start[c + 1]) c++;
+			atomicAdd(&ctl[c].alive, 1);
+		}
+	}
+}
+
+__global__ void __launch_bounds__(256) tick_store_kernel(const ReqDev* reqs, const RunRef* work, const TickRun* runs, int n)
+{
+	for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < n; w += gridDim.x * blockDim.x)
+		reqs[work[w].req].next[work[w].run] = runs[w].next;
 }
 
 // --------------------------------------------------------------------------
@@ -352,9 +484,6 @@ struct Request {
 	bool done = false;
 	int natoms = 0, ntors = 0;
 	double t_submit = 0, t_done = 0;
-	// per run: tasks (kind | index bits of the task word) still queued when a
-	// tick's time ran out; they open the run's part of the next tick
-	std::vector<std::vector<uint32_t>> leftover;
 	// result processing inputs (host copies from the prepared ligand)
 	PostLigand post;
 	std::vector<uint32_t> pairs;
@@ -376,15 +505,13 @@ struct Engine {
 	uint64_t next_id = 1;
 	cudaStream_t stream = nullptr;
 	ReqDev* d_reqs = nullptr; int d_reqs_cap = 0;
-	// per-tick device buffers, grown on demand: work items, their done flags,
-	// phase counters and quotas; the task rings and their control blocks
+	// per-tick device buffers, grown on demand: work items, their phase
+	// counters and done flags; the classes' control blocks
 	RunRef* d_work = nullptr; int d_work_cap = 0;
+	TickRun* d_runs = nullptr;
 	uint8_t* d_done = nullptr;
-	int* d_pending = nullptr;
-	int* d_quota = nullptr;
-	unsigned long long* d_slots = nullptr; size_t d_slots_cap = 0;
 	QueueCtl* d_ctl = nullptr;
-	int ga_chunk = 16;
+	long long idle_ns = kIdleNs;                  // a pose group's idle limit (engine configuration)
 	cudaMemPool_t pool = nullptr;                 // request tables and state, kept by the pool when freed
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;     // around a tick's launches
 	std::vector<uint8_t> h_done;
@@ -401,7 +528,6 @@ struct Engine {
 		if (pool) cudaMemPoolDestroy(pool);
 		if (d_reqs) cudaFree(d_reqs);
 		if (d_work) cudaFree(d_work);
-		if (d_slots) cudaFree(d_slots);
 		if (d_ctl) cudaFree(d_ctl);
 		if (ev0) cudaEventDestroy(ev0);
 		if (ev1) cudaEventDestroy(ev1);
@@ -413,7 +539,7 @@ static size_t request_bytes(int runs, int pop, size_t tables)
 {
 	size_t n = (size_t)runs * pop;
 	return tables + n * kGenotypeStride * 4 * 3 /* conf x2, prng */ + n * 4 * 3 /* e x2, evals_new */ +
-	       (size_t)runs * (4 + 4 + 4 + 3 + 4 + kGenotypeStride * 4) + 1024;
+	       (size_t)runs * (4 + 4 + 4 + 3 + 4 + 8 + kGenotypeStride * 4) + 1024;
 }
 
 // Launches the tick's kernel for local search LSMET.  Its CTAs are split
@@ -486,8 +612,11 @@ adgpu_status adgpu_engine_create(const adgpu_engine_config* cfg, adgpu_engine** 
 	Engine& E = en->e;
 	if (cfg) E.cfg = *cfg;
 	if (E.cfg.gens_per_tick <= 0) E.cfg.gens_per_tick = 1 << 30;
-	if (E.cfg.threads_per_pose != 0 && E.cfg.threads_per_pose != 32 && E.cfg.threads_per_pose != 64 &&
-	    E.cfg.threads_per_pose != 128) { delete en; return fail(ADGPU_ERR_ARG, "threads_per_pose must be 0, 32, 64 or 128"); }
+	if (E.cfg.threads_per_pose != 0 && E.cfg.threads_per_pose != -1 && E.cfg.threads_per_pose != 32 &&
+	    E.cfg.threads_per_pose != 64 && E.cfg.threads_per_pose != 128) {
+		delete en;
+		return fail(ADGPU_ERR_ARG, "threads_per_pose must be -1, 0, 32, 64 or 128");
+	}
 	cudaError_t e = cudaSetDevice(E.cfg.device);
 	if (e != cudaSuccess) { delete en; return cuda_fail(e, "set device"); }
 	size_t fr = 0, tot = 0;
@@ -496,6 +625,11 @@ adgpu_status adgpu_engine_create(const adgpu_engine_config* cfg, adgpu_engine** 
 	e = cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking);
 	if (e != cudaSuccess) { delete en; return cuda_fail(e, "stream"); }
 	if (E.cfg.tick_ms < 0.0f || E.cfg.tick_ms != E.cfg.tick_ms) { delete en; return fail(ADGPU_ERR_ARG, "tick_ms must be >= 0"); }
+	if (E.cfg.idle_timeout_ms < 0.0f || E.cfg.idle_timeout_ms != E.cfg.idle_timeout_ms) {
+		delete en;
+		return fail(ADGPU_ERR_ARG, "idle_timeout_ms must be >= 0");
+	}
+	if (E.cfg.idle_timeout_ms > 0.0f) E.idle_ns = (long long)(1e6 * (double)E.cfg.idle_timeout_ms);
 	{
 		cudaMemPoolProps props{};
 		props.allocType = cudaMemAllocationTypePinned;
@@ -574,7 +708,8 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 	size_t o_tab = take(pk.blob.size()), o_c0 = take(n * kGenotypeStride * 4), o_c1 = take(n * kGenotypeStride * 4), o_e0 = take(n * 4),
 	       o_e1 = take(n * 4), o_ev = take(n * 4), o_pr = take(n * 64 * 4), o_er = take(runs * 4), o_gen = take(runs * 4),
 	       o_cur = take(runs), o_done = take(runs), o_init = take(runs), o_be = take(runs * 4),
-	       o_bg = take((size_t)runs * kGenotypeStride * 4), o_pend = take((size_t)runs * 4);
+	       o_bg = take((size_t)runs * kGenotypeStride * 4), o_pend = take((size_t)runs * 4),
+	       o_next = take((size_t)runs * 8);
 	cudaError_t e = cudaMallocFromPoolAsync(&r->state, off, E.pool, E.stream);
 	if (e != cudaSuccess) return cuda_fail(e, "request state");
 	char* B = static_cast<char*>(r->state);
@@ -582,6 +717,13 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 	if (e == cudaSuccess) e = cudaMemcpyAsync(B + o_tab, pk.blob.data(), pk.blob.size(), cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(B + o_c0, p.initpop.data(), n * kGenotypeStride * 4, cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(B + o_pr, p.prng.data(), n * 64 * 4, cudaMemcpyHostToDevice, E.stream);
+	// step 0 (scoring the initial population) open: its P entities pending,
+	// none handed out (the phase counters are zero from the memset)
+	if (e == cudaSuccess) {
+		std::vector<int> pend(runs, dp.pop_size);
+		e = cudaMemcpyAsync(B + o_pend, pend.data(), (size_t)runs * 4, cudaMemcpyHostToDevice, E.stream);
+		if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+	}
 	if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
 	if (e != cudaSuccess) { cudaFreeAsync(r->state, E.stream); r->state = nullptr; return cuda_fail(e, "request upload"); }
 	place_ligand(pk, B + o_tab, r->tables.dev);
@@ -608,6 +750,7 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 	d.best_e = reinterpret_cast<float*>(B + o_be);
 	d.best_g = reinterpret_cast<float*>(B + o_bg);
 	d.pending = reinterpret_cast<int*>(B + o_pend);
+	d.next = reinterpret_cast<unsigned long long*>(B + o_next);
 	d.max_evals = rp->max_evals;
 	d.max_gens = rp->max_gens ? rp->max_gens : 0xFFFFFFFFu;
 	d.lsmet = rp->lsmet;
@@ -615,24 +758,22 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 	r->id = E.next_id++;
 	r->receptor = rp->receptor;
 	r->runs = runs;
-	r->leftover.assign(runs, {});
 	r->post = lig->p.post;
 	r->pairs = lig->p.pairs;
 	r->dp = dp;
 	r->bytes = need;
 	r->natoms = dp.num_of_atoms;
 	r->ntors = dp.num_of_genes - 6;
-	if (E.cfg.threads_per_pose) r->tpp = E.cfg.threads_per_pose;
-	else {
-		r->tpp = tune_tpp(E, *r);
-		// Solis-Wets and ADADELTA searches stop on their own test, so every
-		// generation of a run waits for its longest search: two warps per pose
-		// halve that wait, which the steady-state scorer timing cannot see
-		// (64 uneven ligands, nrun 20, ADADELTA: 92.9 k ligands/h at 64 against
-		// 75.2 k with the tuned sizes; serving p50 0.14 s against 0.34 s at 18
-		// requests/s).  ADAM and FIRE run fixed-length searches: tuned size.
-		if ((rp->lsmet == LS_SW || rp->lsmet == LS_AD) && r->tpp < 64) r->tpp = 64;
-	}
+	// threads per pose: the configured size; by default one warp, the size
+	// with the most evaluations per SM (runs advance independently and every
+	// entity is a task of its own, so no generation waits behind a longest
+	// search); -1: the fastest size on a short scoring benchmark of the
+	// ligand.  (64 uneven ligands, nrun 20, ADADELTA: 100 k ligands/h with
+	// 32 for all, 97 k with 64, 76 k with the tuned sizes, whose classes
+	// split the GPU between them.)
+	if (E.cfg.threads_per_pose > 0) r->tpp = E.cfg.threads_per_pose;
+	else if (E.cfg.threads_per_pose < 0) r->tpp = tune_tpp(E, *r);
+	else r->tpp = 32;
 	r->t_submit = now_s();
 	E.used += need;
 	E.stats.submitted++;
@@ -653,7 +794,6 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	std::vector<RunRef> work[NC];
 	int max_atoms[NC], max_tors[NC], max_tasks[NC];
 	double weight[NC];
-	const int chunk = E.ga_chunk;
 	for (int c = 0; c < NC; c++) { max_atoms[c] = 1; max_tors[c] = 0; max_tasks[c] = 1; weight[c] = 0; }
 	for (auto& kv : E.requests) {
 		Request& r = *kv.second;
@@ -666,25 +806,19 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 		const adgpu_dockpars& dp = r.dev.a.dp;
 		max_atoms[cls] = std::max(max_atoms[cls], r.natoms);
 		max_tors[cls] = std::max(max_tors[cls], r.ntors);
-		max_tasks[cls] = std::max({max_tasks[cls], (int)dp.num_of_lsentities, (dp.pop_size + chunk - 1) / chunk});
+		max_tasks[cls] = std::max({max_tasks[cls], (int)dp.num_of_lsentities, dp.pop_size});
 		weight[cls] += (double)r.runs * (r.dev.a.L.npairs + 8.0 * r.natoms + 64.0);
 	}
 	if (completed) *completed = 0;
 	if (reqs.empty()) return ADGPU_OK;
-	size_t nwork = 0, slots = 0;
-	size_t start[NC], cap[NC], slot0[NC];
+	size_t start[NC];
 	std::vector<RunRef> all;
 	for (int c = 0; c < NC; c++) {
 		start[c] = all.size();
 		all.insert(all.end(), work[c].begin(), work[c].end());
-		// a run has at most max_tasks tasks queued at once; twice that keeps a
-		// reserved slot from being reused before its previous lap is read
-		cap[c] = work[c].empty() ? 0 : 2 * work[c].size() * (size_t)max_tasks[c] + 1024;
-		slot0[c] = slots;
-		slots += cap[c];
 	}
-	nwork = all.size();
-	if (nwork >= kMaxTickRuns) return fail(ADGPU_ERR_LIMIT, "more than 524287 runs admitted at once");
+	const size_t nwork = all.size();
+	if (nwork >= (size_t)0x3fffffff) return fail(ADGPU_ERR_LIMIT, "too many runs admitted at once");
 	cudaError_t e;
 	if ((int)reqs.size() > E.d_reqs_cap) {
 		if (E.d_reqs) cudaFree(E.d_reqs);
@@ -695,53 +829,32 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	if ((int)nwork > E.d_work_cap) {
 		if (E.d_work) cudaFree(E.d_work);
 		E.d_work_cap = std::max<int>((int)nwork * 2, 256);
-		const size_t per = sizeof(RunRef) + 2 * sizeof(int) + 1;
+		const size_t per = sizeof(RunRef) + sizeof(TickRun) + 1;
 		e = cudaMalloc(&E.d_work, per * E.d_work_cap + 256);
 		if (e != cudaSuccess) { E.d_work = nullptr; E.d_work_cap = 0; return cuda_fail(e, "work list"); }
 		char* B = reinterpret_cast<char*>(E.d_work) + sizeof(RunRef) * E.d_work_cap;
-		E.d_pending = reinterpret_cast<int*>(B);
-		E.d_quota = E.d_pending + E.d_work_cap;
-		E.d_done = reinterpret_cast<uint8_t*>(E.d_quota + E.d_work_cap);
+		B = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(B) + 15) & ~uintptr_t(15));
+		E.d_runs = reinterpret_cast<TickRun*>(B);
+		E.d_done = reinterpret_cast<uint8_t*>(E.d_runs + E.d_work_cap);
 	}
-	if (slots > E.d_slots_cap) {
-		if (E.d_slots) cudaFree(E.d_slots);
-		E.d_slots_cap = slots * 2;
-		e = cudaMalloc(&E.d_slots, E.d_slots_cap * sizeof(unsigned long long));
-		if (e != cudaSuccess) { E.d_slots = nullptr; E.d_slots_cap = 0; return cuda_fail(e, "task rings"); }
-	}
-	// initial state, queued in each class's ring (lap 1; the rest of the ring
-	// empty, lap 0 matches no position): the tasks a run had still queued when
-	// the previous tick's time ran out, else its START task
-	std::vector<unsigned long long> h_init[NC];
-	std::vector<int> h_quota(nwork, E.cfg.gens_per_tick);
 	QueueCtl h_ctl[NC];
 	memset(h_ctl, 0, sizeof(h_ctl));
+	ClassBounds cb;
 	for (int c = 0; c < NC; c++) {
-		for (size_t i = 0; i < work[c].size(); i++) {
-			const uint32_t w = (uint32_t)(start[c] + i);
-			std::vector<uint32_t>& left = order[work[c][i].req]->leftover[work[c][i].run];
-			if (left.empty()) {
-				h_init[c].push_back((1ull << 32) | task_word(w, kTaskStart, 0));
-			} else {
-				for (uint32_t kind_idx : left) h_init[c].push_back((1ull << 32) | (w << (kTaskIdxBits + 2)) | kind_idx);
-				left.clear();
-			}
-		}
-		h_ctl[c].tail = h_init[c].size();
-		h_ctl[c].alive = (int)work[c].size();
+		h_ctl[c].alive = 0;                  // counted by tick_load_kernel
 		h_ctl[c].t_first = ~0ull;
+		cb.start[c] = (int)start[c];
 	}
+	cb.start[NC] = (int)nwork;
 	e = cudaMemcpyAsync(E.d_reqs, reqs.data(), sizeof(ReqDev) * reqs.size(), cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_work, all.data(), sizeof(RunRef) * nwork, cudaMemcpyHostToDevice, E.stream);
-	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_quota, h_quota.data(), sizeof(int) * nwork, cudaMemcpyHostToDevice, E.stream);
-	if (e == cudaSuccess) e = cudaMemsetAsync(E.d_done, 0, nwork, E.stream);
-	if (e == cudaSuccess) e = cudaMemsetAsync(E.d_slots, 0, slots * sizeof(unsigned long long), E.stream);
-	for (int c = 0; c < NC && e == cudaSuccess; c++)
-		if (!h_init[c].empty())
-			e = cudaMemcpyAsync(E.d_slots + slot0[c], h_init[c].data(), h_init[c].size() * sizeof(unsigned long long),
-			                    cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_ctl, h_ctl, sizeof(h_ctl), cudaMemcpyHostToDevice, E.stream);
 	if (e != cudaSuccess) return cuda_fail(e, "tick upload");
+	const int lgrid = (int)std::min<size_t>((nwork + 255) / 256, 1024);
+	tick_load_kernel<<<lgrid, 256, 0, E.stream>>>(E.d_reqs, E.d_work, E.d_runs, E.d_done, (int)nwork, E.cfg.gens_per_tick,
+	                                              E.d_ctl, cb);
+	e = cudaGetLastError();
+	if (e != cudaSuccess) return cuda_fail(e, "tick load");
 	if (!E.ev0) { cudaEventCreate(&E.ev0); cudaEventCreate(&E.ev1); }
 	cudaEventRecord(E.ev0, E.stream);
 	for (int m = 0; m < 4; m++) {
@@ -750,17 +863,15 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 		bool any = false;
 		TickArgs t;
 		memset(&t, 0, sizeof(t));
-		t.reqs = E.d_reqs; t.work = E.d_work; t.work_done = E.d_done;
-		t.quota = E.d_quota; t.ga_chunk = chunk;
+		t.reqs = E.d_reqs; t.work = E.d_work; t.runs = E.d_runs; t.work_done = E.d_done;
 		t.tick_ns = (long long)(1e6 * (double)E.cfg.tick_ms);
+		t.idle_ns = E.idle_ns;
 		for (int k = 0; k < 3; k++) {
 			const int c = k * 4 + m;
 			nr[k] = (int)work[c].size(); ma[k] = max_atoms[c]; mt[k] = max_tors[c]; mx[k] = max_tasks[c]; wt[k] = weight[c];
-			t.cls[k].slots = E.d_slots + slot0[c];
 			t.cls[k].ctl = E.d_ctl + c;
-			t.cls[k].cap = (uint32_t)cap[c];
-			t.cls[k].slot_spin = kSlotSpin;
-			t.cls[k].idle_ns = kIdleNs;
+			t.cls[k].w0 = (int)start[c];
+			t.cls[k].nw = nr[k];
 			any |= nr[k] > 0;
 		}
 		if (!any) continue;
@@ -774,6 +885,11 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 		if (st != ADGPU_OK) return st;
 	}
 	cudaEventRecord(E.ev1, E.stream);
+	// the runs' phase counters back into their requests' state: a phase
+	// begun in this tick continues in the next
+	tick_store_kernel<<<lgrid, 256, 0, E.stream>>>(E.d_reqs, E.d_work, E.d_runs, (int)nwork);
+	e = cudaGetLastError();
+	if (e != cudaSuccess) return cuda_fail(e, "tick store");
 	E.h_done.resize(nwork);
 	e = cudaMemcpyAsync(E.h_done.data(), E.d_done, nwork, cudaMemcpyDeviceToHost, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(h_ctl, E.d_ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, E.stream);
@@ -781,26 +897,10 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	if (e != cudaSuccess) return cuda_fail(e, "engine tick");
 	const bool timed = E.cfg.tick_ms > 0.0f;
 	for (int c = 0; c < NC; c++) {
-		if (h_ctl[c].err) return fail(ADGPU_ERR_TIMEOUT, "engine task queue: a reserved slot was never written");
+		if (h_ctl[c].err)
+			return fail(ADGPU_ERR_TIMEOUT, "engine tick: pose groups found no task for the idle limit while runs were "
+			                               "still active (a phase whose tasks never completed)");
 		if (h_ctl[c].alive != 0 && !timed) return fail(ADGPU_ERR_STATE, "engine tick ended with runs still active");
-		// tasks left queued when the tick's time ran out go back to their runs
-		if (timed && h_ctl[c].tail > h_ctl[c].head) {
-			const unsigned long long h = h_ctl[c].head, n = h_ctl[c].tail - h;
-			if (n > cap[c]) return fail(ADGPU_ERR_STATE, "engine task ring overran");
-			std::vector<unsigned long long> left(n);
-			const unsigned long long first = std::min<unsigned long long>(n, cap[c] - h % cap[c]);
-			e = cudaMemcpy(left.data(), E.d_slots + slot0[c] + h % cap[c], first * 8, cudaMemcpyDeviceToHost);
-			if (e == cudaSuccess && n > first)
-				e = cudaMemcpy(left.data() + first, E.d_slots + slot0[c], (n - first) * 8, cudaMemcpyDeviceToHost);
-			if (e != cudaSuccess) return cuda_fail(e, "queued tasks");
-			for (unsigned long long k = 0; k < n; k++) {
-				const uint64_t v = left[k];
-				if ((v >> 32) != (h + k) / cap[c] + 1) return fail(ADGPU_ERR_STATE, "engine task ring: unwritten slot after the tick");
-				const uint32_t tw = (uint32_t)v, w = tw >> (kTaskIdxBits + 2);
-				if (w >= nwork) return fail(ADGPU_ERR_STATE, "engine task ring: bad run index");
-				order[all[w].req]->leftover[all[w].run].push_back(tw & ((1u << (kTaskIdxBits + 2)) - 1));
-			}
-		}
 		if (h_ctl[c].workers > 0 && h_ctl[c].t_last > h_ctl[c].t_first) {
 			E.stats.worker_busy_s += 1e-9 * (double)h_ctl[c].busy_ns;
 			E.stats.worker_span_s += 1e-9 * (double)h_ctl[c].workers * (double)(h_ctl[c].t_last - h_ctl[c].t_first);
@@ -825,6 +925,42 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	E.stats.completed += comp;
 	if (completed) *completed = comp;
 	return ADGPU_OK;
+}
+
+adgpu_status adgpu_engine_cancel(adgpu_engine* en, uint64_t request_id)
+{
+	if (!en) return fail(ADGPU_ERR_ARG, "null engine");
+	Engine& E = en->e;
+	std::lock_guard<std::mutex> lk(E.mu);
+	auto it = E.requests.find(request_id);
+	if (it == E.requests.end()) return fail(ADGPU_ERR_ARG, "unknown request");
+	Request& r = *it->second;
+	if (r.state) cudaFreeAsync(r.state, E.stream);
+	r.state = nullptr;
+	E.used -= r.bytes;
+	E.stats.cancelled++;
+	E.requests.erase(it);
+	return ADGPU_OK;
+}
+
+adgpu_status adgpu_engine_inject_stall(adgpu_engine* en, uint64_t request_id)
+{
+	if (!en) return fail(ADGPU_ERR_ARG, "null engine");
+	Engine& E = en->e;
+	std::lock_guard<std::mutex> lk(E.mu);
+	auto it = E.requests.find(request_id);
+	if (it == E.requests.end()) return fail(ADGPU_ERR_ARG, "unknown request");
+	Request& r = *it->second;
+	if (r.done) return fail(ADGPU_ERR_STATE, "request already finished");
+	// every entity of each run's open phase handed out, none completed
+	std::vector<unsigned long long> next(r.runs);
+	cudaError_t e = cudaMemcpyAsync(next.data(), r.dev.next, (size_t)r.runs * 8, cudaMemcpyDeviceToHost, E.stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+	if (e != cudaSuccess) return cuda_fail(e, "stall read");
+	for (auto& v : next) v = (v & 0xffffffff00000000ull) | 0xffffffull;
+	e = cudaMemcpyAsync(r.dev.next, next.data(), (size_t)r.runs * 8, cudaMemcpyHostToDevice, E.stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+	return e == cudaSuccess ? ADGPU_OK : cuda_fail(e, "stall write");
 }
 
 adgpu_status adgpu_engine_run(adgpu_engine* en)

@@ -471,15 +471,19 @@ __device__ __forceinline__ void ga_block(const KArgs& a, uint32_t b, const Group
 
 // Initial population energies (cuda/kernel1.cu:26-55).
 template <int TPP>
-__device__ void initpop_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+__device__ void initpop_block(const KArgs& a, const PopBufs& pb, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
 {
 	const int NG = a.dp.num_of_genes;
-	for (int k = G.rank; k < NG; k += TPP) S.gen[k] = a.conf[(size_t)b * kGenotypeStride + k];
+	for (int k = G.rank; k < NG; k += TPP) S.gen[k] = pb.conf[(size_t)b * kGenotypeStride + k];
 	G.sync();
 	const float e = score_pose<TPP, false>(a.L, S.gen, nullptr, S.pose, G);
-	if (G.rank == 0) { a.e[b] = e; a.evals_new[b] = 1; }
+	if (G.rank == 0) { pb.e[b] = e; a.evals_new[b] = 1; }
 	G.sync();
 }
+
+template <int TPP>
+__device__ __forceinline__ void initpop_block(const KArgs& a, uint32_t b, const Group<TPP>& G, const GroupSmem& S)
+{ initpop_block<TPP>(a, bufs_of(a), b, G, S); }
 
 // Stand-alone scorer: energies (and gradients when a.conf_cur != nullptr is
 // used as the gradient output) of nblocks genotypes.

@@ -414,17 +414,25 @@ bool pipeline_applies(const adgpu_dockpars& dp, uint32_t runs)
 	       dp.pop_size <= (1 << kPipeRunShift) && runs > 0 && runs < (1u << (31 - kPipeRunShift));
 }
 
-// Threads per pose of the pipelined loop: 32 for every local search.  Runs
-// advance independently and a generation's entities are handed out oldest
-// generation first, so the launch no longer ends each generation with its
-// longest searches running alone (the reason the per-generation launches use
-// 64 for Solis-Wets and ADADELTA), and one warp per pose gives the most
-// evaluations per SM (B200, cfg2, 100 runs: ADADELTA 158 vs 148, Solis-Wets
-// 255 vs 249, ADAM 174 vs 155, FIRE 140 vs 119 M evals/s against 64).
-int pipeline_default_tpp(int lsmet)
+// Threads per pose of the pipelined loop: the smallest group that still has
+// about four entities per pose group in a generation (runs * pop_size tasks
+// over SMs x 6 CTAs x 128/TPP groups).  Runs advance independently and a
+// generation's entities are handed out oldest generation first, so a launch
+// no longer ends each generation with its longest searches running alone,
+// and one warp per pose gives the most evaluations per SM when there is work
+// for all of them (B200, cfg2, 100 runs: ADADELTA 158 vs 148, Solis-Wets 255
+// vs 249, ADAM 174 vs 155, FIRE 140 vs 119 M evals/s against 64).  With few
+// runs a run's chain of generations decides, and larger groups shorten it
+// (16 uneven ligands of 20 runs, ADADELTA: 54, 86 and 102 M evals/s at 32,
+// 64 and 128).
+int pipeline_default_tpp(int lsmet, long tasks)
 {
 	(void)lsmet;
-	return 32;
+	int dev = 0, sms = 148;
+	if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	for (int tpp = 32; tpp < 128; tpp *= 2)
+		if (tasks >= 4L * sms * ADGPU_MIN_CTAS * (kPipeThreads / tpp)) return tpp;
+	return 128;
 }
 
 // Population buffers (look-ahead + 1): with 32 threads per pose a run's
@@ -446,7 +454,7 @@ adgpu_status dock_pipelined(const KArgs& base, PipeScratch& sc, int lsmet, int t
 {
 	const adgpu_dockpars& dp = base.dp;
 	if (!pipeline_applies(dp, runs)) return fail(ADGPU_ERR_ARG, "pipelined docking needs a 100 % local-search rate");
-	if (tpp == 0) tpp = pipeline_default_tpp(lsmet);
+	if (tpp == 0) tpp = pipeline_default_tpp(lsmet, (long)runs * dp.pop_size);
 	if (tpp != 32 && tpp != 64 && tpp != 128) return fail(ADGPU_ERR_ARG, "threads per pose must be 32, 64 or 128");
 	const int P = dp.pop_size;
 	const size_t n = (size_t)runs * P;

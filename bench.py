@@ -750,7 +750,7 @@ def run_serve(args):
             "ligands_per_hour": 3600.0 * nreq / t_total, "latency_p50_s": float(np.percentile(lat, 50)),
             "latency_p99_s": float(np.percentile(lat, 99)), "memory_budget_gb": args.budget_gb,
             "gens_per_tick": args.gens_per_tick, "tick_ms": args.tick_ms, "ticks": int(en.stats().ticks),
-            "results_processed_on_device": bool(args.process_results), "threads_per_pose": args.engine_tpp or "tuned",
+            "results_processed_on_device": bool(args.process_results), "threads_per_pose": {0: 32, -1: "tuned"}.get(args.engine_tpp, args.engine_tpp),
             "host_seconds": {"submit": t_submit, "tick": t_tick, "results": t_result, "total": t_total,
                              "engine_kernels": en.stats().kernel_s},
             "worker_utilisation": (en.stats().worker_busy_s / en.stats().worker_span_s
@@ -856,8 +856,8 @@ def main():
     ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel / loop-kernel modes)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
     ap.add_argument("--engine-tpp", type=int, default=0,
-                    help="engine threads per pose (batch / serve modes): 0 = automatic (tuned per ligand size, "
-                         "at least 64 for sw/ad), or 32, 64, 128")
+                    help="engine threads per pose (batch / serve modes): 0 = the engine's default (32), "
+                         "-1 = tuned per ligand size, or 32, 64, 128")
     ap.add_argument("--nlig", type=int, default=64, help="ligands (batch mode)")
     ap.add_argument("--batch-config", type=int, default=3, choices=[3, 4],
                     help="batch mode workload: 3 (uneven ligands) or 4 (80^3 maps, 2 flexible residues, nrun 50)")

@@ -460,9 +460,10 @@ adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_ref
  * states on the device until its result is taken.  adgpu_engine_tick
  * advances every admitted run by up to gens_per_tick generations, or until
  * tick_ms has passed, in one persistent launch per local-search method whose
- * pose groups take tasks (GA chunks, single local searches) from device
- * queues; between ticks requests can be submitted and results taken
- * (continuous batching).  Each run stops on its own budget (evals >=
+ * pose groups take tasks (one entity of a run's generation: its GA step and
+ * its local search) from the runs' own counters, least advanced run first;
+ * between ticks requests can be submitted and results taken (continuous
+ * batching).  Each run stops on its own budget (evals >=
  * max_evals or generations >= max_gens), so a request's result does not
  * depend on what else is running or on where ticks end.
  * ------------------------------------------------------------------------- */
@@ -470,10 +471,12 @@ typedef struct adgpu_engine_s adgpu_engine;
 
 typedef struct {
 	size_t memory_budget_bytes;  /* device bytes for receptors + requests; 0: 80% of free memory */
-	int    threads_per_pose;     /* 32, 64 or 128; 0: tuned per ligand size class */
+	int    threads_per_pose;     /* 32, 64 or 128; 0: 32; -1: tuned per ligand size class */
 	int    gens_per_tick;        /* generations per tick; <= 0: run every admitted run to completion */
 	int    device;               /* CUDA device ordinal */
-	float  tick_ms;              /* > 0: a tick also ends after this long: runs take no new GA phase after it */
+	float  tick_ms;              /* > 0: a tick also ends after this long: no pose group takes a new task after it */
+	float  idle_timeout_ms;      /* a pose group that finds no task for this long while runs are active ends
+	                                the tick with ADGPU_ERR_TIMEOUT; 0: 2000 */
 } adgpu_engine_config;
 
 typedef struct {
@@ -484,7 +487,7 @@ typedef struct {
 } adgpu_request_params;
 
 typedef struct {
-	uint64_t submitted, completed, ticks;
+	uint64_t submitted, completed, cancelled, ticks;
 	size_t   bytes_used, bytes_budget;
 	int      active;
 	/* Worker accounting over all ticks: time pose groups spent on tasks, and
@@ -509,6 +512,15 @@ adgpu_status adgpu_engine_tick(adgpu_engine* engine, int* completed);
 /* Ticks until every admitted request has finished. */
 adgpu_status adgpu_engine_run(adgpu_engine* engine);
 adgpu_status adgpu_engine_poll(adgpu_engine* engine, uint64_t request_id, int* done);
+/* Drops a request between ticks, finished or not, and frees its device
+ * state (no result is kept). */
+adgpu_status adgpu_engine_cancel(adgpu_engine* engine, uint64_t request_id);
+/* Failure injection for tests: every run of the request stops handing out
+ * tasks, as if all of its open phase had been taken by pose groups that never
+ * finish, so the next tick's pose groups find nothing to do while the runs
+ * stay active and the tick returns ADGPU_ERR_TIMEOUT after idle_timeout_ms
+ * (the device-side wait limit at work).  adgpu_engine_cancel clears it. */
+adgpu_status adgpu_engine_inject_stall(adgpu_engine* engine, uint64_t request_id);
 /* Result of a finished request (any output may be NULL): best energy and
  * genotype of each run's final population, evals and generations per run,
  * submit-to-finish latency.  Frees the request's device state. */

@@ -84,10 +84,15 @@ def test_batch_uneven_ligands_and_mix_invariance(grid, tpp):
 
 
 def test_automatic_threads_per_pose(grid):
-    """Without a configured size: the tuned size per ligand-size bucket, at
-    least 64 for the searches that stop on their own test (Solis-Wets,
-    ADADELTA), whose phases wait for their longest search."""
-    en = engine.Engine()
+    """Tuned sizes (threads_per_pose -1): the size picked per ligand-size
+    bucket, the same for every request of a bucket whatever its local
+    search; the default is one warp per pose."""
+    assert engine.Engine().submit is not None
+    d = engine.Engine()
+    drec = d.add_receptor(grid)
+    assert d.info(d.submit(ligand(grid, 3, 20, 6, runs=2), drec, "ad", max_evals=5_000))[0] == 32
+    d.close()
+    en = engine.Engine(threads_per_pose=-1)
     rec = en.add_receptor(grid)
     lg = ligand(grid, 3, 20, 6, runs=2)
     got = {}
@@ -95,8 +100,8 @@ def test_automatic_threads_per_pose(grid):
         rid = en.submit(lg, rec, m, max_evals=5_000)
         got[m] = en.info(rid)[0]
     en.run()
-    assert got["sw"] >= 64 and got["ad"] >= 64
     assert all(v in (32, 64, 128) for v in got.values())
+    assert len(set(got.values())) == 1
     en.close()
 
 
