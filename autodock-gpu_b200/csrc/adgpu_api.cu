@@ -16,6 +16,12 @@
 #ifndef ADGPU_MIN_CTAS
 #define ADGPU_MIN_CTAS 6     // 6 CTAs x 4 warps per SM: <= 80 registers, no spills
 #endif
+// The gradient local searches (ADADELTA, ADAM, FIRE) need more registers than
+// 80 for their scorer without spills; the SM's throughput is the same with 5
+// CTAs as with 6 (the scorer is issue bound).
+#ifndef ADGPU_MIN_CTAS_GRAD
+#define ADGPU_MIN_CTAS_GRAD 5
+#endif
 
 namespace adgpu {
 
@@ -38,8 +44,10 @@ adgpu_status cuda_fail(cudaError_t e, const char* what)
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
+constexpr int lga_min_ctas(int kind) { return kind >= 2 && kind <= 4 ? ADGPU_MIN_CTAS_GRAD : ADGPU_MIN_CTAS; }
+
 template <int TPP, int KIND>
-__global__ void __launch_bounds__(128, ADGPU_MIN_CTAS) lga_kernel(KArgs a, float* grads)
+__global__ void __launch_bounds__(128, lga_min_ctas(KIND)) lga_kernel(KArgs a, float* grads)
 {
 	if (a.stop_flag && *a.stop_flag) return;
 	int gid, ngroups;
@@ -173,7 +181,7 @@ adgpu_status launch_lga(const KArgs& a, float* grads, cudaStream_t stream, int c
 	auto kfn = lga_kernel<TPP, KIND>;
 	if (bytes > 48 * 1024) ADGPU_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "smem attribute");
 	static int carveout = -2;           // per instantiation: the last preference set
-	const int pct = smem_carveout_pct(bytes, ADGPU_MIN_CTAS);
+	const int pct = smem_carveout_pct(bytes, lga_min_ctas(KIND));
 	if (pct >= 0 && pct > carveout) {
 		ADGPU_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, pct), "carveout");
 		carveout = pct;

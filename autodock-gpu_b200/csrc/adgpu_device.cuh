@@ -39,8 +39,9 @@ constexpr int kMaxGenes = 63;
 constexpr int kGenotypeStride = 64;
 
 // ---- repacked per-ligand tables --------------------------------------------------
-// Pair record: the type-pair parameters and the charge/desolvation prefactors
-// of one intramolecular contributor, so the pair loop reads 32 contiguous bytes.
+// Pair record of a pair with other exponents than the AD4 force field's
+// (modified pair potentials): the type-pair parameters and the
+// charge/desolvation prefactors of one intramolecular contributor, 32 bytes.
 struct __align__(16) PairRec {
 	float ac, bd, reqm, dsolv_pref;   // VWpars_AC, VWpars_BD, reqm_AB, (S1+qasp|q1|)V2+(S2+qasp|q2|)V1
 	float qq;                         // coeff_elec*q1*q2
@@ -48,6 +49,56 @@ struct __align__(16) PairRec {
 	uint32_t ij;                      // atom1 | atom2<<8 | m<<16 | n<<24
 	uint32_t pad;
 };
+
+// Two pairs of the AD4 force field (exponents m = 12 and n = 6 or 10), the
+// ones one thread takes in one step of the pair loop: pair A of an aligned
+// group of 32 pairs (one warp instruction) and pair B of the next group,
+// 64 bytes in four quads whose fields interleave A and B, so packed FP32x2
+// instructions take both pairs' operands straight from the loaded registers:
+//   q0 = (AC_A, AC_B, b6_A, b6_B)     VWpars_AC; VWpars_BD of a 12-6 pair, else 0
+//   q1 = (b10_A, b10_B, reqm_A, reqm_B)  VWpars_BD of a 12-10 pair, else 0; reqm_AB
+//   q2 = (ds_A, ds_B, qq_A, qq_B)     coeff_desolv*((S1+qasp|q1|)V2 + (S2+qasp|q2|)V1); coeff_elec*q1*q2
+//   q3 = (G_A, G_B, ij_A, ij_B)       G of a CG-G0 pair, else 0; atom1 | atom2 << 8
+// With BD in b6 or b10 by the pair's n (the other 0) the vdW/H-bond energy is
+// AC/sd^12 - b6/sd^6 - b10/sd^10 with no select.  The 32 records of a group
+// pair are stored quad by quad (quad j of record r at float4 index
+// (r/32)*128 + j*32 + r%32), so a warp's load of one quad reads 512
+// contiguous bytes.  Padding entries (lists are whole group pairs) have every
+// coefficient 0 and both atoms the same: they add exactly 0 to energies and
+// forces.
+__host__ __device__ inline uint32_t pair2_quad(uint32_t rec, uint32_t j) { return (rec / 32u) * 128u + j * 32u + rec % 32u; }
+
+// Slot (record, half) of the s-th pair of the ordered list of AD4 pairs:
+// group s/32 is half (s/32) % 2 of records (s/64)*32 .. +31, lane s % 32.
+__host__ __device__ inline void pair2_slot(uint32_t s, uint32_t* rec, uint32_t* half)
+{
+	*rec = (s / 64u) * 32u + (s % 32u);
+	*half = (s / 32u) & 1u;
+}
+// Records for n ordered AD4 pairs (whole groups of 64 pairs, padded).
+__host__ __device__ inline uint32_t pair2_records(uint32_t n) { return (n + 63u) / 64u * 32u; }
+
+// Writes one pair into half h of record rec (quads Q).
+__host__ __device__ inline void pair2_set(float4* Q, uint32_t rec, uint32_t h, float ac, float b6, float b10, float reqm,
+                                          float ds, float qq, float vb, uint32_t ij)
+{
+	float* q0 = reinterpret_cast<float*>(Q + pair2_quad(rec, 0));
+	float* q1 = reinterpret_cast<float*>(Q + pair2_quad(rec, 1));
+	float* q2 = reinterpret_cast<float*>(Q + pair2_quad(rec, 2));
+	float* q3 = reinterpret_cast<float*>(Q + pair2_quad(rec, 3));
+	q0[h] = ac; q0[2 + h] = b6;
+	q1[h] = b10; q1[2 + h] = reqm;
+	q2[h] = ds; q2[2 + h] = qq;
+	q3[h] = vb; reinterpret_cast<uint32_t*>(q3)[2 + h] = ij;
+}
+// A padding record (both halves) for lane position rec % 32 of an N-atom
+// ligand: the atoms are spread so that padded lanes do not all hit one
+// shared-memory bank.
+__host__ __device__ inline void pair2_pad(float4* Q, uint32_t rec, uint32_t N)
+{
+	const uint32_t a = (rec % 32u) % N;
+	for (uint32_t h = 0; h < 2; h++) pair2_set(Q, rec, h, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, a | (a << 8));
+}
 
 // Stored position of element p of a list of n (torsion items; pairs in the
 // kernel-API repack of adgpu_noalloc.cu) in warp-interleaved order.  The reference lists pairs by first atom and items
@@ -66,8 +117,10 @@ __host__ __device__ inline uint32_t interleave_pos(uint32_t p, uint32_t n)
 }
 
 struct LigDev {
-	// sizes
+	// sizes (npairs: all intramolecular pairs; npairs2: two-pair records of
+	// the AD4 pairs; ngpairs: pairs with other exponents)
 	int natoms, nlig, ngenes, ntors, npairs, ntoritems;
+	int npairs2, ngpairs;
 	int map_e;                   // index of the e map in the cell record (0)
 	// grid
 	int gx, gy, gz;              // grid points per axis
@@ -84,7 +137,8 @@ struct LigDev {
 	const float4* tors_mv;       // rotatable bond moving vectors
 	const int2* tors_ends;       // rotatable bond atom pair
 	const uint32_t* tor_items;   // (torsion<<8 | atom) per rotating atom, grouped by torsion
-	const PairRec* pairs;
+	const float4* pairs2;        // AD4 pairs, two per record (quads, pair2_quad)
+	const PairRec* gpairs;       // pairs with other exponents
 	const float* grid;           // cell records, 32-byte aligned
 };
 
@@ -222,12 +276,15 @@ struct Group {
 
 // ---- per-pose shared-memory scratch -------------------------------------------------
 // Layout (natoms rounded up to a multiple of 4):
-//   tq [ntors] float4; xyz [N] float4 (x, y, z, 0); fx, fy, fz [N] int; gg [64] int
+//   tq [ntors] float4; xyz [N] float4 (x, y, z, 0); f3 [3N] int; gg [64] int
 // An atom's coordinates are one 16-byte load, so a pair reads both its atoms
-// with two shared-memory loads.
+// with two shared-memory loads.  Its fixed-point force is f3[3a .. 3a+2]:
+// one address per atom for the three components, and since 3 is odd, atoms
+// whose indices differ mod 32 fall in different banks, as in three separate
+// arrays.
 struct PoseSmem {
 	float4* xyz;
-	int* fx; int* fy; int* fz;
+	int* f3;
 	float4* tq;
 	float2* gsc;       // sin/cos of theta, phi and half the rotation angle
 	int* gg;
@@ -250,9 +307,8 @@ __device__ __forceinline__ PoseSmem carve_pose(char* base, int natoms, int ntors
 	f += 8;
 	s.xyz = reinterpret_cast<float4*>(f);         // still 16-byte aligned
 	f += 4 * n4;
-	s.fx = reinterpret_cast<int*>(f);
-	s.fy = s.fx + n4; s.fz = s.fy + n4;
-	s.gg = s.fz + n4;
+	s.f3 = reinterpret_cast<int*>(f);
+	s.gg = s.f3 + 3 * n4;
 	return s;
 }
 
@@ -284,15 +340,17 @@ __device__ __forceinline__ GenRot genrot_from(const float* g, bool has_ligand, c
 
 // ---- intramolecular pairs, two per thread with packed FP32 -------------------------
 // sm_100 executes FADD2/FMUL2/FFMA2: one instruction on two floats.  The pair
-// loop is issue bound, so each thread takes two pairs per iteration and runs
-// their shared arithmetic packed; compares, selects, reciprocals and the
-// fixed-point atomics stay per pair.
+// loop is issue bound, so each thread takes two pairs per step and runs their
+// arithmetic packed; compares, reciprocals and the fixed-point atomics stay
+// per pair.
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 f2neg(float2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b, exactly (one rounding of -1*b + a)
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) { return __ffma2_rn(f2s(-1.0f), b, a); }
+__device__ __forceinline__ float2 f2rcp(float2 a) { return f2(__fdividef(1.0f, a.x), __fdividef(1.0f, a.y)); }
 // 1.0f where a < b, else 0.0f (one FSET, no predicate and select)
 __device__ __forceinline__ float lt1(float a, float b)
 {
@@ -309,127 +367,114 @@ static __device__ __noinline__ float pow_int(float b, int e)
 	return r;
 }
 
-// Energy of the pairs this thread takes (rank, rank + TPP, rank + 2*TPP, ...),
-// with, for GRAD, their fixed-point forces added to S.fx/fy/fz.  The terms
-// are the reference's (cuda/calcMergeEneGra.cu:418-602) rewritten with one
-// reciprocal square root and three reciprocals per pair instead of divisions
-// and __powf:  (AC - sd^(m-n) BD) sd^-m = AC/sd^m - BD/sd^n  (m = 12, n = 6 or 10).
+// The fixed-point force of one pair (components already scaled by 1024):
+// -q on the first atom, +q on the second (f3: three ints per atom).
+__device__ __forceinline__ void pair_force(int* f3, uint32_t i, uint32_t j, float gx, float gy, float gz)
+{
+	const int ix = quant_scaled(gx), iy = quant_scaled(gy), iz = quant_scaled(gz);
+	int* fi = f3 + 3 * i;
+	int* fj = f3 + 3 * j;
+	atomicAdd(fi, -ix); atomicAdd(fi + 1, -iy); atomicAdd(fi + 2, -iz);
+	atomicAdd(fj, ix); atomicAdd(fj + 1, iy); atomicAdd(fj + 2, iz);
+}
+
+// Energy of the AD4 pairs this thread takes (records rank, rank + TPP, ...),
+// with, for GRAD, their fixed-point forces added to S.f3.  The terms are the
+// reference's (cuda/calcMergeEneGra.cu:418-602) rewritten with one reciprocal
+// square root and three reciprocals per pair instead of divisions and __powf:
+// (AC - sd^(m-n) BD) sd^-m = AC/sd^12 - BD/sd^n; the smoothed distance
+// (|reqm - r| >= hs ? r + copysign(hs, reqm - r) : reqm) as reqm clamped to
+// [r - hs, r + hs], the elec_min_distance floor as a max (and a min on 1/r).
 // TERMS (energy only): also adds this thread's vdW/H-bond, electrostatic,
 // desolvation and CG-G0 sums to tsum[0..3].
 template <int TPP, bool GRAD, bool TERMS = false>
 __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, int rank, float* tsum = nullptr)
 {
-	constexpr uint32_t k12_6 = 12u | (6u << 8), k12_10 = 12u | (10u << 8);
 	// loop invariants read once: when L lives in shared memory (the engine's
 	// per-task arguments) the force atomics below would otherwise force a
 	// reload of every field in every iteration
 	const float hs = L.half_smooth, emd = L.elec_min_distance;
 	const float inv_emd = __fdividef(1.0f, emd);
-	const int npairs = L.npairs;
-	const PairRec* const pairs = L.pairs;
-	const float spacing = L.spacing, inv_spacing = L.inv_spacing, coeff_desolv = L.coeff_desolv;
+	const int nrec = L.npairs2;
+	const float spacing = L.spacing, inv_spacing = L.inv_spacing;
+	const float4* const xyz = S.xyz;
+	int* const f3 = S.f3;
 	float2 esum = f2s(0.0f);
 	float2 t_vdw = f2s(0.0f), t_el = f2s(0.0f), t_ds = f2s(0.0f), t_cg = f2s(0.0f);
-	for (int p = rank; p < npairs; p += 2 * TPP) {
-		const bool has_b = p + TPP < npairs;          // the second pair; else pair a twice, b discarded
-		const float4* pra = reinterpret_cast<const float4*>(pairs + p);
-		const float4* prb = reinterpret_cast<const float4*>(pairs + (has_b ? p + TPP : p));
-		const float4 Aa = __ldg(pra), Ba = __ldg(pra + 1), Ab = __ldg(prb), Bb = __ldg(prb + 1);
-		const uint32_t ija = __float_as_uint(Ba.z), ijb = __float_as_uint(Bb.z);
-		const int a1 = ija & 0xFF, a2 = (ija >> 8) & 0xFF, b1 = ijb & 0xFF, b2 = (ijb >> 8) & 0xFF;
-		const float4 pa1 = S.xyz[a1], pa2 = S.xyz[a2], pb1 = S.xyz[b1], pb2 = S.xyz[b2];
-		const float2 sx = f2add(f2(pa1.x, pb1.x), f2(-pa2.x, -pb2.x));
-		const float2 sy = f2add(f2(pa1.y, pb1.y), f2(-pa2.y, -pb2.y));
-		const float2 sz = f2add(f2(pa1.z, pb1.z), f2(-pa2.z, -pb2.z));
+	// record d = rank + TPP*i: quads at pair2_quad(d, j); the pointer steps
+	// TPP/32 blocks of 128 quads per iteration
+	const float4* pr = L.pairs2 + (rank / 32) * 128 + (rank % 32);
+	for (int d = rank; d < nrec; d += TPP, pr += (TPP / 32) * 128) {
+		const float4 q0 = __ldg(pr), q1 = __ldg(pr + 32), q2 = __ldg(pr + 64), q3 = __ldg(pr + 96);
+		const uint32_t ija = __float_as_uint(q3.z), ijb = __float_as_uint(q3.w);
+		const uint32_t a1 = ija & 0xFFu, a2 = ija >> 8, b1 = ijb & 0xFFu, b2 = ijb >> 8;
+		const float4 pa1 = xyz[a1], pa2 = xyz[a2], pb1 = xyz[b1], pb2 = xyz[b2];
+		const float2 sx = f2(pa1.x - pa2.x, pb1.x - pb2.x);
+		const float2 sy = f2(pa1.y - pa2.y, pb1.y - pb2.y);
+		const float2 sz = f2(pa1.z - pa2.z, pb1.z - pb2.z);
 		const float2 d2g = f2fma(sz, sz, f2fma(sy, sy, f2mul(sx, sx)));
 		// coincident atoms (d2g = 0) get r = 0 from a finite reciprocal
 		const float2 inv_dist = f2(rsqrtf(fmaxf(d2g.x, 1e-30f)), rsqrtf(fmaxf(d2g.y, 1e-30f)));
 		const float2 r = f2mul(f2mul(d2g, inv_dist), f2s(spacing));
-		const float2 vbond = f2(Ba.y, Bb.y);          // G for CG-G0 pairs, else 0
-		float2 e = f2mul(vbond, r);
-		float2 pg = vbond;
-		if constexpr (TERMS) t_cg = f2add(t_cg, f2mul(f2(1.0f, has_b ? 1.0f : 0.0f), f2mul(vbond, r)));
+		const float2 vb = f2(q3.x, q3.y);             // G for CG-G0 pairs, else 0
+		float2 e = f2mul(vb, r);
+		float2 pg = vb;
+		if constexpr (TERMS) t_cg = f2add(t_cg, e);
 		// vdW / H-bond, cut-off 8 A
 		{
-			const float2 reqm = f2(Aa.z, Ab.z);
-			const float2 delta = f2add(reqm, f2neg(r));
-			float2 sd;
-			sd.x = fabsf(delta.x) >= hs ? r.x + copysignf(hs, delta.x) : reqm.x;
-			sd.y = fabsf(delta.y) >= hs ? r.y + copysignf(hs, delta.y) : reqm.y;
-			const float2 inv = f2(__fdividef(1.0f, sd.x), __fdividef(1.0f, sd.y));
+			const float2 lo = f2add(r, f2s(-hs)), hi = f2add(r, f2s(hs));
+			const float2 sd = f2(fminf(fmaxf(q1.z, lo.x), hi.x), fminf(fmaxf(q1.w, lo.y), hi.y));
+			const float2 inv = f2rcp(sd);
 			const float2 i2 = f2mul(inv, inv), i4 = f2mul(i2, i2), i6 = f2mul(i4, i2);
-			float2 im = f2mul(i6, i6), in_, fm = f2s(12.0f), fn;
-			const uint32_t mna = ija >> 16, mnb = ijb >> 16;
-			if ((mna == k12_6 || mna == k12_10) && (mnb == k12_6 || mnb == k12_10)) {
-				const float2 i10 = f2mul(i6, i4);
-				in_.x = mna == k12_10 ? i10.x : i6.x;
-				in_.y = mnb == k12_10 ? i10.y : i6.y;
-				fn.x = mna == k12_10 ? 10.0f : 6.0f;
-				fn.y = mnb == k12_10 ? 10.0f : 6.0f;
-			} else {
-				const int ma = mna & 0xFF, na = mna >> 8, mb = mnb & 0xFF, nb = mnb >> 8;
-				im = f2(pow_int(inv.x, ma), pow_int(inv.y, mb));
-				in_ = f2(pow_int(inv.x, na), pow_int(inv.y, nb));
-				fm = f2((float)ma, (float)mb);
-				fn = f2((float)na, (float)nb);
-			}
-			const float2 ac = f2(Aa.x, Ab.x), bd = f2(Aa.y, Ab.y);
-			const float2 bd_in = f2mul(bd, in_), ac_im = f2mul(ac, im);
-			const float2 ev = f2add(ac_im, f2neg(bd_in));
+			const float2 t12 = f2mul(f2(q0.x, q0.y), f2mul(i6, i6));
+			const float2 t6 = f2mul(f2(q0.z, q0.w), i6);
+			const float2 t10 = f2mul(f2(q1.x, q1.y), f2mul(i6, i4));
+			const float2 ev = f2sub(f2sub(t12, t6), t10);
 			// cut-off as a 0/1 factor: the terms are finite for every r (sd >= r - hs)
 			const float2 in8 = f2(lt1(r.x, 8.0f), lt1(r.y, 8.0f));
 			e = f2fma(in8, ev, e);
-			if constexpr (TERMS) t_vdw = f2add(t_vdw, f2mul(f2(1.0f, has_b ? 1.0f : 0.0f), f2mul(in8, ev)));
+			if constexpr (TERMS) t_vdw = f2add(t_vdw, f2mul(in8, ev));
 			if (GRAD) {
-				const float2 gv = f2mul(f2add(f2mul(fn, bd_in), f2neg(f2mul(fm, ac_im))), inv);
+				// d/dsd: (6 b6/sd^6 + 10 b10/sd^10 - 12 AC/sd^12) / sd
+				const float2 gv = f2mul(f2fma(f2s(6.0f), t6, f2fma(f2s(10.0f), t10, f2mul(f2s(-12.0f), t12))), inv);
 				pg = f2fma(in8, gv, pg);
 			}
 		}
 		// electrostatics and desolvation, cut-off 20.48 A
 		{
 			const float2 in20 = f2(lt1(r.x, 20.48f), lt1(r.y, 20.48f));
-			float2 inv_r = f2mul(inv_dist, f2s(inv_spacing));
-			float2 rr = r;
-			if (rr.x < emd) { rr.x = emd; inv_r.x = inv_emd; }
-			if (rr.y < emd) { rr.y = emd; inv_r.y = inv_emd; }
+			const float2 rr = f2(fmaxf(r.x, emd), fmaxf(r.y, emd));
+			const float2 ir = f2mul(inv_dist, f2s(inv_spacing));
+			const float2 inv_r = f2(fminf(ir.x, inv_emd), fminf(ir.y, inv_emd));
 			const float2 d2 = f2mul(rr, rr);
 			const float2 num = f2fma(f2mul(f2s(-0.1063f), d2), f2fma(f2s(-0.001947f), d2, f2s(1.0f)), f2s(12.96f));
 			const float2 den = f2fma(d2, f2fma(d2, f2fma(f2s(0.000112f), d2, f2s(0.00357f)), f2s(0.4137f)), f2s(12.96f));
-			const float2 cn = f2mul(f2s(coeff_desolv), num);
-			const float2 desolv = f2mul(f2(Aa.w, Ab.w), f2(__fdividef(cn.x, den.x), __fdividef(cn.y, den.y)));
-			const float2 rs = f2(__fdividef(1.0f, rr.x + 1.26366f), __fdividef(1.0f, rr.y + 1.26366f));
+			const float2 desolv = f2mul(f2mul(f2(q2.x, q2.y), num), f2rcp(den));
+			const float2 rs = f2rcp(f2add(rr, f2s(1.26366f)));
 			const float2 rs2 = f2mul(rs, rs);
 			const float2 diel = f2fma(f2s(1.10859f), rs2, f2s(0.010358f));
-			const float2 es = f2mul(f2(Ba.x, Bb.x), inv_r);
+			const float2 es = f2mul(f2(q2.z, q2.w), inv_r);
 			const float2 ee = f2fma(diel, es, desolv);
 			e = f2fma(in20, ee, e);
 			if constexpr (TERMS) {
-				const float2 bm = f2(1.0f, has_b ? 1.0f : 0.0f);
-				t_el = f2add(t_el, f2mul(bm, f2mul(in20, f2mul(diel, es))));
-				t_ds = f2add(t_ds, f2mul(bm, f2mul(in20, desolv)));
+				t_el = f2add(t_el, f2mul(in20, f2mul(diel, es)));
+				t_ds = f2add(t_ds, f2mul(in20, desolv));
 			}
 			if (GRAD) {
-				const float2 t1 = f2mul(f2mul(es, inv_r), diel);
-				const float2 t2 = f2mul(f2mul(f2mul(es, f2s(2.21718f)), rs2), rs);
-				const float2 t3 = f2mul(f2mul(f2s(0.0771605f), rr), desolv);
-				const float2 ge = f2add(f2add(t1, t2), t3);
-				pg = f2fma(f2neg(in20), ge, pg);
+				// es (diel / r + 2.21718 rs^3) + 0.0771605 r desolv
+				const float2 ge = f2fma(es, f2fma(inv_r, diel, f2mul(f2mul(f2s(2.21718f), rs2), rs)),
+				                        f2mul(f2mul(f2s(0.0771605f), rr), desolv));
+				pg = f2fma(f2s(-1.0f), f2mul(in20, ge), pg);
 			}
 		}
-		esum = f2add(esum, f2(e.x, has_b ? e.y : 0.0f));
+		esum = f2add(esum, e);
 		if (GRAD) {
 			// fixed-point forces; the 1024 scale folded into gdd (a power of two:
 			// the same rounding as quant(sub * gdd))
-			const float2 gdd = f2mul(f2mul(f2neg(pg), inv_dist), f2s(kTermScale));
+			const float2 gdd = f2mul(pg, f2mul(inv_dist, f2s(-kTermScale)));
 			const float2 gx = f2mul(sx, gdd), gy = f2mul(sy, gdd), gz = f2mul(sz, gdd);
-			int ix = quant_scaled(gx.x), iy = quant_scaled(gy.x), iz = quant_scaled(gz.x);
-			atomicAdd(&S.fx[a1], -ix); atomicAdd(&S.fy[a1], -iy); atomicAdd(&S.fz[a1], -iz);
-			atomicAdd(&S.fx[a2], ix); atomicAdd(&S.fy[a2], iy); atomicAdd(&S.fz[a2], iz);
-			if (has_b) {
-				ix = quant_scaled(gx.y); iy = quant_scaled(gy.y); iz = quant_scaled(gz.y);
-				atomicAdd(&S.fx[b1], -ix); atomicAdd(&S.fy[b1], -iy); atomicAdd(&S.fz[b1], -iz);
-				atomicAdd(&S.fx[b2], ix); atomicAdd(&S.fy[b2], iy); atomicAdd(&S.fz[b2], iz);
-			}
+			pair_force(f3, a1, a2, gx.x, gy.x, gz.x);
+			pair_force(f3, b1, b2, gx.y, gy.y, gz.y);
 		}
 	}
 	if constexpr (TERMS) {
@@ -439,6 +484,57 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 		tsum[3] += t_cg.x + t_cg.y;
 	}
 	return esum.x + esum.y;
+}
+
+// Pairs with other exponents than 12-6 / 12-10 (modified pair potentials;
+// the AD4 front end has none), one per thread, the reference's terms with
+// sd^-m and sd^-n by repeated squaring.
+template <int TPP, bool GRAD, bool TERMS = false>
+__device__ __forceinline__ float pair_terms_generic(const LigDev& L, const PoseSmem& S, int rank, float* tsum = nullptr)
+{
+	const float hs = L.half_smooth, emd = L.elec_min_distance;
+	float esum = 0.0f;
+	for (int p = rank; p < L.ngpairs; p += TPP) {
+		const PairRec P = L.gpairs[p];
+		const uint32_t a1 = P.ij & 0xFFu, a2 = (P.ij >> 8) & 0xFFu;
+		const int m = (int)((P.ij >> 16) & 0xFFu), n = (int)(P.ij >> 24);
+		const float4 p1 = S.xyz[a1], p2 = S.xyz[a2];
+		const float sx = p1.x - p2.x, sy = p1.y - p2.y, sz = p1.z - p2.z;
+		const float d2g = sx * sx + sy * sy + sz * sz;
+		const float inv_dist = rsqrtf(fmaxf(d2g, 1e-30f));
+		const float r = d2g * inv_dist * L.spacing;
+		float e = P.vbond * r, pg = P.vbond;
+		if constexpr (TERMS) tsum[3] += e;
+		if (r < 8.0f) {
+			const float sd = fminf(fmaxf(P.reqm, r - hs), r + hs);
+			const float inv = __fdividef(1.0f, sd);
+			const float im = pow_int(inv, m), in_ = pow_int(inv, n);
+			const float ev = P.ac * im - P.bd * in_;
+			e += ev;
+			if constexpr (TERMS) tsum[0] += ev;
+			if (GRAD) pg += ((float)n * P.bd * in_ - (float)m * P.ac * im) * inv;
+		}
+		if (r < 20.48f) {
+			const float rr = fmaxf(r, emd);
+			const float inv_r = fminf(inv_dist * L.inv_spacing, __fdividef(1.0f, emd));
+			const float d2 = rr * rr;
+			const float num = (-0.1063f * d2) * (-0.001947f * d2 + 1.0f) + 12.96f;
+			const float den = d2 * (d2 * (0.000112f * d2 + 0.00357f) + 0.4137f) + 12.96f;
+			const float desolv = P.dsolv_pref * __fdividef(L.coeff_desolv * num, den);
+			const float rs = __fdividef(1.0f, rr + 1.26366f);
+			const float diel = 1.10859f * rs * rs + 0.010358f;
+			const float es = P.qq * inv_r;
+			e += diel * es + desolv;
+			if constexpr (TERMS) { tsum[1] += diel * es; tsum[2] += desolv; }
+			if (GRAD) pg -= es * (inv_r * diel + 2.21718f * rs * rs * rs) + 0.0771605f * rr * desolv;
+		}
+		esum += e;
+		if (GRAD) {
+			const float gdd = -pg * inv_dist * kTermScale;
+			pair_force(S.f3, a1, a2, sx * gdd, sy * gdd, sz * gdd);
+		}
+	}
+	return esum;
 }
 
 // ---- the scorer -----------------------------------------------------------------------
@@ -561,20 +657,24 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 				}
 			}
 		}
-		if (GRAD) { S.fx[a] = fx; S.fy[a] = fy; S.fz[a] = fz; }
+		if (GRAD) { int* fa = S.f3 + 3 * a; fa[0] = fx; fa[1] = fy; fa[2] = fz; }
 	}
 	G.sync();
 
 	// 4. intramolecular pairs (cuda/calcMergeEneGra.cu:418-602)
 	if constexpr (TERMS) e_acc += pair_terms<TPP, GRAD, TERMS>(L, S, rank, tt + 3);
 	else e_acc += pair_terms<TPP, GRAD>(L, S, rank);
+	if (L.ngpairs > 0) {
+		if constexpr (TERMS) e_acc += pair_terms_generic<TPP, GRAD, TERMS>(L, S, rank, tt + 3);
+		else e_acc += pair_terms_generic<TPP, GRAD>(L, S, rank);
+	}
 	if constexpr (TERMS) {
 		G.template sum_n<8>(tt);
 		if (rank == 0)
 			for (int k = 0; k < 8; k++) terms[k] = tt[k];
 	}
 	if (!GRAD) return G.sum(e_acc);
-	G.sync();   // every pair's forces are in S.fx/fy/fz
+	G.sync();   // every pair's forces are in S.f3
 
 	// 5. torque and total force over the ligand atoms (cuda/calcMergeEneGra.cu:608-661);
 	//    the energy rides along as a seventh sum (one cross-warp exchange, not two)
@@ -582,7 +682,8 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	for (int a = rank; a < L.nlig; a += TPP) {
 		const float4 pa = S.xyz[a];
 		float3 r = make_float3((pa.x - gr.mv.x) * L.spacing, (pa.y - gr.mv.y) * L.spacing, (pa.z - gr.mv.z) * L.spacing);
-		float3 f = make_float3(kOneOverTermScale * (float)S.fx[a], kOneOverTermScale * (float)S.fy[a], kOneOverTermScale * (float)S.fz[a]);
+		const int* fa = S.f3 + 3 * a;
+		float3 f = make_float3(kOneOverTermScale * (float)fa[0], kOneOverTermScale * (float)fa[1], kOneOverTermScale * (float)fa[2]);
 		red[3] += f.x; red[4] += f.y; red[5] += f.z;
 		float3 t = cross3(r, f);
 		red[0] += t.x; red[1] += t.y; red[2] += t.z;
@@ -629,7 +730,8 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 		float l = rnorm3df(ux, uy, uz);
 		ux *= l; uy *= l; uz *= l;
 		float3 r = make_float3(pl.x - rx, pl.y - ry, pl.z - rz);
-		float3 f = make_float3(kOneOverTermScale * (float)S.fx[la], kOneOverTermScale * (float)S.fy[la], kOneOverTermScale * (float)S.fz[la]);
+		const int* fl = S.f3 + 3 * la;
+		float3 f = make_float3(kOneOverTermScale * (float)fl[0], kOneOverTermScale * (float)fl[1], kOneOverTermScale * (float)fl[2]);
 		float3 t = cross3(r, f);
 		float on_axis = (ux * t.x + uy * t.y + uz * t.z) * L.spacing;
 		atomicAdd(&S.gg[6 + k], quant(on_axis * kDegToRad));

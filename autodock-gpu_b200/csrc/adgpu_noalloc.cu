@@ -33,6 +33,7 @@ namespace {
 
 struct NoAllocLayout {
 	size_t ligdev = 0, status = 0, xyzq = 0, info = 0, clen = 0, chain = 0, uv = 0, mv = 0, ends = 0, items = 0, pairs = 0;
+	size_t pairs_bytes = 0;      // two-pair records of the AD4 pairs from the front, PairRec entries from the back
 	size_t total = 0;
 };
 
@@ -53,7 +54,10 @@ NoAllocLayout layout_for(const adgpu_dockpars& dp)
 	l.mv = o; o = up16(o + (NT + 1) * 16);
 	l.ends = o; o = up16(o + (NT + 1) * 8);
 	l.items = o; o = up16(o + N * (NT + 1) * 4);
-	l.pairs = o; o = up16(o + Q * sizeof(PairRec));
+	// AD4 pairs take pair2_records(Qs) * 64 <= 32 * Qs + 2048 bytes and the
+	// others 32 * Qg, so this holds any split of the Q pairs
+	l.pairs = o; l.pairs_bytes = (size_t)pair2_records((uint32_t)Q) * 64 + 32 * 64;
+	o = up16(o + l.pairs_bytes);
 	l.total = o;
 	return l;
 }
@@ -152,37 +156,74 @@ __global__ void __launch_bounds__(256) noalloc_repack_kernel(adgpu_gpudata d, Li
 			items[interleave_pos((uint32_t)(s_istart[k] + c), (uint32_t)s_istart[NT])] = ((uint32_t)k << 8) | (uint32_t)la;
 		}
 	}
-	// intramolecular pairs
+	// intramolecular pairs: the AD4 ones (m = 12, n = 6 or 10) into
+	// two-pair records in warp-interleaved order (interleave_pos), the others one to
+	// a PairRec; each thread takes a contiguous chunk, and a scan of the
+	// per-chunk counts of other-exponent pairs gives every pair its index
 	const uint32_t* pairs = d.pKerconst_intracontrib->intraE_contributors_const;
 	const adgpu_kc_intra* kin = d.pKerconst_intra;
-	PairRec* pr = reinterpret_cast<PairRec*>(base + lay.pairs);
 	const uint32_t nat = (uint32_t)dp.num_of_atypes;
-	for (int p = threadIdx.x; p < Q; p += blockDim.x) {
-		uint32_t a1 = pairs[2 * p], a2 = pairs[2 * p + 1];
+	__shared__ int s_gen[257];
+	const int chunk = (Q + (int)blockDim.x - 1) / (int)blockDim.x;
+	const int p0 = min(Q, (int)threadIdx.x * chunk), p1 = min(Q, p0 + chunk);
+	auto exps_of = [&](int p, uint32_t& a1, uint32_t& a2, uint32_t& t1, uint32_t& t2) {
+		a1 = pairs[2 * p]; a2 = pairs[2 * p + 1];
 		if (a1 >= (uint32_t)N || a2 >= (uint32_t)N) { status[0] = 1; a1 = a2 = 0; }
-		uint32_t t1 = ii->atom_types_const[a1], t2 = ii->atom_types_const[a2];
+		t1 = ii->atom_types_const[a1]; t2 = ii->atom_types_const[a2];
 		if (t1 >= nat || t2 >= nat) { status[0] = 1; t1 = t2 = 0; }
-		uint32_t idx = t1 * nat + t2;
-		unsigned short exps = kin->VWpars_exp_const[idx];
-		uint32_t m = (exps & 0xFF00) >> 8, n = exps & 0xFF;
-		uint32_t h1 = kin->atom_types_reqm_const[t1], h2 = kin->atom_types_reqm_const[t2];
-		bool cgg0 = (h1 == 24 && h2 == 25) || (h1 == 25 && h2 == 24);
-		float q1 = ii->atom_charges_const[a1], q2 = ii->atom_charges_const[a2];
-		PairRec r;
-		r.ac = kin->VWpars_AC_const[idx];
-		r.bd = kin->VWpars_BD_const[idx];
-		r.reqm = kin->reqm_AB_const[idx];
-		r.dsolv_pref = __fadd_rn(__fmul_rn(__fadd_rn(kin->dspars_S_const[t1], __fmul_rn(dp.qasp, fabsf(q1))), kin->dspars_V_const[t2]),
-		                         __fmul_rn(__fadd_rn(kin->dspars_S_const[t2], __fmul_rn(dp.qasp, fabsf(q2))), kin->dspars_V_const[t1]));
-		r.qq = __fmul_rn(__fmul_rn(dp.coeff_elec, q1), q2);
-		r.vbond = cgg0 ? 50.0f : 0.0f;
-		r.ij = a1 | (a2 << 8) | (m << 16) | (n << 24);
-		r.pad = 0;
-		pr[interleave_pos((uint32_t)p, (uint32_t)Q)] = r;
+		return (uint32_t)kin->VWpars_exp_const[t1 * nat + t2];
+	};
+	auto is_ad4 = [](uint32_t exps) { const uint32_t m = (exps & 0xFF00) >> 8, n = exps & 0xFF; return m == 12 && (n == 6 || n == 10); };
+	int ngen = 0;
+	for (int p = p0; p < p1; p++) {
+		uint32_t a1, a2, t1, t2;
+		if (!is_ad4(exps_of(p, a1, a2, t1, t2))) ngen++;
+	}
+	s_gen[threadIdx.x + 1] = ngen;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		s_gen[0] = 0;
+		for (int i = 0; i < (int)blockDim.x; i++) s_gen[i + 1] += s_gen[i];
+	}
+	__syncthreads();
+	const int Qg = s_gen[blockDim.x], Qs = Q - Qg;
+	const uint32_t nrec = pair2_records((uint32_t)Qs);
+	float4* pr2 = reinterpret_cast<float4*>(base + lay.pairs);
+	PairRec* gpr = reinterpret_cast<PairRec*>(base + lay.pairs + lay.pairs_bytes - (size_t)Qg * sizeof(PairRec));
+	for (uint32_t r = threadIdx.x; r < nrec; r += blockDim.x) pair2_pad(pr2, r, (uint32_t)N);
+	__syncthreads();
+	int gi = s_gen[threadIdx.x];
+	for (int p = p0; p < p1; p++) {
+		uint32_t a1, a2, t1, t2;
+		const uint32_t exps = exps_of(p, a1, a2, t1, t2);
+		const uint32_t m = (exps & 0xFF00) >> 8, n = exps & 0xFF;
+		const uint32_t idx = t1 * nat + t2;
+		const uint32_t h1 = kin->atom_types_reqm_const[t1], h2 = kin->atom_types_reqm_const[t2];
+		const bool cgg0 = (h1 == 24 && h2 == 25) || (h1 == 25 && h2 == 24);
+		const float q1 = ii->atom_charges_const[a1], q2 = ii->atom_charges_const[a2];
+		const float ac = kin->VWpars_AC_const[idx], bd = kin->VWpars_BD_const[idx], reqm = kin->reqm_AB_const[idx];
+		const float dsp = __fadd_rn(__fmul_rn(__fadd_rn(kin->dspars_S_const[t1], __fmul_rn(dp.qasp, fabsf(q1))), kin->dspars_V_const[t2]),
+		                            __fmul_rn(__fadd_rn(kin->dspars_S_const[t2], __fmul_rn(dp.qasp, fabsf(q2))), kin->dspars_V_const[t1]));
+		const float qq = __fmul_rn(__fmul_rn(dp.coeff_elec, q1), q2);
+		const float vb = cgg0 ? 50.0f : 0.0f;
+		if (is_ad4(exps)) {
+			uint32_t rec, h;
+			pair2_slot(interleave_pos((uint32_t)(p - gi), (uint32_t)Qs), &rec, &h);
+			pair2_set(pr2, rec, h, ac, n == 6 ? bd : 0.0f, n == 10 ? bd : 0.0f, reqm, __fmul_rn(dp.coeff_desolv, dsp), qq,
+			          vb, a1 | (a2 << 8));
+		} else {
+			PairRec r;
+			r.ac = ac; r.bd = bd; r.reqm = reqm; r.dsolv_pref = dsp; r.qq = qq; r.vbond = vb;
+			r.ij = a1 | (a2 << 8) | (m << 16) | (n << 24);
+			r.pad = 0;
+			gpr[gi++] = r;
+		}
 	}
 	__syncthreads();
 	if (threadIdx.x == 0) {
 		L.ntoritems = s_istart[NT];
+		L.npairs2 = (int)nrec; L.ngpairs = Qg;
+		L.pairs2 = pr2; L.gpairs = gpr;
 		*reinterpret_cast<LigDev*>(base + lay.ligdev) = L;
 	}
 }
@@ -268,7 +309,6 @@ extern "C" adgpu_status adgpu_score_genotypes_noalloc(const adgpu_gpudata* data,
 	L.tors_mv = reinterpret_cast<const float4*>(base + lay.mv);
 	L.tors_ends = reinterpret_cast<const int2*>(base + lay.ends);
 	L.tor_items = reinterpret_cast<const uint32_t*>(base + lay.items);
-	L.pairs = reinterpret_cast<const PairRec*>(base + lay.pairs);
 	L.gx = dp.gridsize_x; L.gy = dp.gridsize_y; L.gz = dp.gridsize_z;
 	L.cells_x = dp.gridsize_x - 1;
 	L.cells_xy = (dp.gridsize_x - 1) * (dp.gridsize_y - 1);

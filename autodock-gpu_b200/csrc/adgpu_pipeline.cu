@@ -47,8 +47,17 @@
 #include "adgpu_queue.cuh"
 #include "adgpu_pipeline.h"
 
-#ifndef ADGPU_MIN_CTAS
-#define ADGPU_MIN_CTAS 6
+// CTAs per SM the persistent kernel is compiled for.  Gradient local
+// searches: 5 CTAs of 4 pose groups; with 6 the SM's throughput is the same
+// (the scorer is issue bound), but the cfg2 ADADELTA docking's 100 runs x
+// 150 entities then leave runs waiting for the stop test (pose groups 95 %
+// busy against 99 %, 158 against 165 M evaluations/s on B200).  Solis-Wets
+// scores energies only, in fewer registers, and gains from the extra warps.
+#ifndef ADGPU_PIPE_MIN_CTAS
+#define ADGPU_PIPE_MIN_CTAS 5
+#endif
+#ifndef ADGPU_PIPE_MIN_CTAS_SW
+#define ADGPU_PIPE_MIN_CTAS_SW 7
 #endif
 
 namespace adgpu {
@@ -317,8 +326,10 @@ __device__ void pipe_worker(const PipeArgs& p)
 	}
 }
 
+constexpr int pipe_min_ctas(int lsmet) { return lsmet == LS_SW ? ADGPU_PIPE_MIN_CTAS_SW : ADGPU_PIPE_MIN_CTAS; }
+
 template <int TPP, int LSMET>
-__global__ void __launch_bounds__(kPipeThreads, ADGPU_MIN_CTAS) pipe_kernel(const PipeArgs p)
+__global__ void __launch_bounds__(kPipeThreads, pipe_min_ctas(LSMET)) pipe_kernel(const PipeArgs p)
 {
 	pipe_worker<TPP, LSMET>(p);
 }
@@ -389,7 +400,7 @@ static adgpu_status launch_pipe(PipeArgs p, long long* d_out, cudaStream_t st)
 	const int gpc = kPipeThreads / TPP;
 	const int bytes = p.group_bytes * gpc;
 	if (bytes > 48 * 1024) ADGPU_CUDA_RET(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "pipeline smem");
-	const int pct = smem_carveout_pct(bytes, ADGPU_MIN_CTAS);
+	const int pct = smem_carveout_pct(bytes, pipe_min_ctas(LSMET));
 	if (pct >= 0) ADGPU_CUDA_RET(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, pct), "pipeline carveout");
 	int per_sm = 0, dev = 0, sms = 0;
 	ADGPU_CUDA_RET(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kPipeThreads, bytes), "pipeline occupancy");
@@ -431,7 +442,7 @@ int pipeline_default_tpp(int lsmet, long tasks)
 	int dev = 0, sms = 148;
 	if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	for (int tpp = 32; tpp < 128; tpp *= 2)
-		if (tasks >= 4L * sms * ADGPU_MIN_CTAS * (kPipeThreads / tpp)) return tpp;
+		if (tasks >= 4L * sms * ADGPU_PIPE_MIN_CTAS * (kPipeThreads / tpp)) return tpp;
 	return 128;
 }
 

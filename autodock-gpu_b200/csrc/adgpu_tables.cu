@@ -148,7 +148,31 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 	out.off_tors_mv = o; o = align_up(o + (size_t)std::max(NT, 1) * 16, 16);
 	out.off_tors_ends = o; o = align_up(o + (size_t)std::max(NT, 1) * 8, 16);
 	out.off_tor_items = o; o = align_up(o + std::max<size_t>(items.size(), 1) * 4, 16);
-	out.off_pairs = o; o = align_up(o + (size_t)std::max(Q, 1) * sizeof(PairRec), 16);
+	// intramolecular pairs: the AD4 ones (m = 12, n = 6 or 10) into
+	// two-pair records (pair2_set), the others (modified pair potentials) one to a PairRec
+	const int nat = dp.num_of_atypes;
+	std::vector<uint32_t> std_pairs;          // (a1, a2) of the AD4 pairs
+	std::vector<int> std_idx, gen_idx;        // their indices in the reference's list
+	for (int p = 0; p < Q; p++) {
+		uint32_t a1 = pairs[2 * p], a2 = pairs[2 * p + 1];
+		if (a1 >= (uint32_t)N || a2 >= (uint32_t)N) return fail(ADGPU_ERR_ARG, "intramolecular pair atom out of range");
+		uint32_t t1 = ii.atom_types_const[a1], t2 = ii.atom_types_const[a2];
+		if (t1 >= (uint32_t)nat || t2 >= (uint32_t)nat) return fail(ADGPU_ERR_ARG, "atom type out of range");
+		unsigned short exps = kin.VWpars_exp_const[t1 * (uint32_t)nat + t2];
+		uint32_t m = (exps & 0xFF00) >> 8, n = exps & 0xFF;
+		if (m == 12 && (n == 6 || n == 10)) {
+			std_idx.push_back(p);
+			std_pairs.push_back(a1);
+			std_pairs.push_back(a2);
+		} else {
+			gen_idx.push_back(p);
+		}
+	}
+	const int Qs = (int)std_idx.size(), Qg = (int)gen_idx.size();
+	out.npairs2 = (int)pair2_records((uint32_t)Qs);
+	out.ngpairs = Qg;
+	out.off_pairs2 = o; o = align_up(o + (size_t)std::max(out.npairs2, 1) * 64, 16);
+	out.off_gpairs = o; o = align_up(o + (size_t)std::max(Qg, 1) * sizeof(PairRec), 16);
 	out.blob.assign(o, 0);
 	uint8_t* B = out.blob.data();
 
@@ -182,33 +206,50 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 	// bank-spread groups of 32 (order_pairs)
 	uint32_t* it_out = reinterpret_cast<uint32_t*>(B + out.off_tor_items);
 	for (size_t i = 0; i < items.size(); i++) it_out[interleave_pos((uint32_t)i, (uint32_t)items.size())] = items[i];
-	PairRec* pr = reinterpret_cast<PairRec*>(B + out.off_pairs);
-	const int nat = dp.num_of_atypes;
-	std::vector<uint32_t> ppos;
-	std::vector<uint8_t> pswap;
-	order_pairs(pairs, Q, ppos, pswap);
-	for (int p = 0; p < Q; p++) {
+	// pair terms in the reference's operand order: desolvation prefactor,
+	// Coulomb factor; G = 50 for CG-G0 pairs (ATYPE_CG_IDX 24 / ATYPE_G0_IDX 25)
+	auto fields = [&](int p, float& ac, float& bd, float& reqm, float& dsolv_pref, float& qq, float& vbond) {
 		uint32_t a1 = pairs[2 * p], a2 = pairs[2 * p + 1];
-		if (a1 >= (uint32_t)N || a2 >= (uint32_t)N) return fail(ADGPU_ERR_ARG, "intramolecular pair atom out of range");
 		uint32_t t1 = ii.atom_types_const[a1], t2 = ii.atom_types_const[a2];
 		uint32_t idx = t1 * (uint32_t)nat + t2;
-		unsigned short exps = kin.VWpars_exp_const[idx];
-		uint32_t m = (exps & 0xFF00) >> 8, n = exps & 0xFF;
 		uint32_t h1 = kin.atom_types_reqm_const[t1], h2 = kin.atom_types_reqm_const[t2];
-		bool cgg0 = (h1 == 24 && h2 == 25) || (h1 == 25 && h2 == 24);   // ATYPE_CG_IDX / ATYPE_G0_IDX
+		bool cgg0 = (h1 == 24 && h2 == 25) || (h1 == 25 && h2 == 24);
 		float q1 = ii.atom_charges_const[a1], q2 = ii.atom_charges_const[a2];
+		ac = kin.VWpars_AC_const[idx];
+		bd = kin.VWpars_BD_const[idx];
+		reqm = kin.reqm_AB_const[idx];
+		dsolv_pref = (kin.dspars_S_const[t1] + dp.qasp * std::fabs(q1)) * kin.dspars_V_const[t2] +
+		             (kin.dspars_S_const[t2] + dp.qasp * std::fabs(q2)) * kin.dspars_V_const[t1];
+		qq = dp.coeff_elec * q1 * q2;
+		vbond = cgg0 ? 50.0f : 0.0f;
+	};
+	float4* pr2 = reinterpret_cast<float4*>(B + out.off_pairs2);
+	for (int r = 0; r < out.npairs2; r++) pair2_pad(pr2, (uint32_t)r, (uint32_t)N);
+	std::vector<uint32_t> ppos;
+	std::vector<uint8_t> pswap;
+	order_pairs(std_pairs.data(), Qs, ppos, pswap);
+	for (int i = 0; i < Qs; i++) {
+		const int p = std_idx[i];
+		uint32_t a1 = pairs[2 * p], a2 = pairs[2 * p + 1];
+		const uint32_t n = kin.VWpars_exp_const[ii.atom_types_const[a1] * (uint32_t)nat + ii.atom_types_const[a2]] & 0xFF;
+		float ac, bd, reqm, dsp, qq, vb;
+		fields(p, ac, bd, reqm, dsp, qq, vb);
+		uint32_t rec, h;
+		pair2_slot(ppos[i], &rec, &h);
+		pair2_set(pr2, rec, h, ac, n == 6 ? bd : 0.0f, n == 10 ? bd : 0.0f, reqm, dp.coeff_desolv * dsp, qq, vb,
+		          pswap[i] ? (a2 | (a1 << 8)) : (a1 | (a2 << 8)));
+	}
+	PairRec* gpr = reinterpret_cast<PairRec*>(B + out.off_gpairs);
+	for (int i = 0; i < Qg; i++) {
+		const int p = gen_idx[i];
+		uint32_t a1 = pairs[2 * p], a2 = pairs[2 * p + 1];
+		unsigned short exps = kin.VWpars_exp_const[ii.atom_types_const[a1] * (uint32_t)nat + ii.atom_types_const[a2]];
+		uint32_t m = (exps & 0xFF00) >> 8, n = exps & 0xFF;
 		PairRec r;
-		r.ac = kin.VWpars_AC_const[idx];
-		r.bd = kin.VWpars_BD_const[idx];
-		r.reqm = kin.reqm_AB_const[idx];
-		// same operand order as the reference's desolvation and Coulomb terms
-		r.dsolv_pref = (kin.dspars_S_const[t1] + dp.qasp * std::fabs(q1)) * kin.dspars_V_const[t2] +
-		               (kin.dspars_S_const[t2] + dp.qasp * std::fabs(q2)) * kin.dspars_V_const[t1];
-		r.qq = dp.coeff_elec * q1 * q2;
-		r.vbond = cgg0 ? 50.0f : 0.0f;
-		r.ij = (pswap[p] ? (a2 | (a1 << 8)) : (a1 | (a2 << 8))) | (m << 16) | (n << 24);
+		fields(p, r.ac, r.bd, r.reqm, r.dsolv_pref, r.qq, r.vbond);
+		r.ij = a1 | (a2 << 8) | (m << 16) | (n << 24);
 		r.pad = 0;
-		pr[ppos[p]] = r;
+		gpr[i] = r;
 	}
 	return ADGPU_OK;
 }
@@ -240,7 +281,9 @@ void place_ligand(const PackedLigand& p, const void* dbase, LigDev& L)
 	L.tors_mv = reinterpret_cast<const float4*>(D + p.off_tors_mv);
 	L.tors_ends = reinterpret_cast<const int2*>(D + p.off_tors_ends);
 	L.tor_items = reinterpret_cast<const uint32_t*>(D + p.off_tor_items);
-	L.pairs = reinterpret_cast<const PairRec*>(D + p.off_pairs);
+	L.npairs2 = p.npairs2; L.ngpairs = p.ngpairs;
+	L.pairs2 = reinterpret_cast<const float4*>(D + p.off_pairs2);
+	L.gpairs = reinterpret_cast<const PairRec*>(D + p.off_gpairs);
 }
 
 void set_grid_fields(LigDev& L, const adgpu_dockpars& dp, const float* cell_grid)

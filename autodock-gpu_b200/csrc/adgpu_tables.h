@@ -17,9 +17,10 @@ adgpu_status cuda_fail(cudaError_t e, const char* what);
 // Host-side packed tables of one ligand (offsets are into `blob`).
 struct PackedLigand {
 	int natoms = 0, nlig = 0, ngenes = 0, ntors = 0, npairs = 0, ntoritems = 0;
+	int npairs2 = 0, ngpairs = 0;     // two-pair records (AD4 pairs), PairRec entries (other exponents)
 	std::vector<uint8_t> blob;
 	size_t off_atom_xyzq = 0, off_atom_info = 0, off_chain_len = 0, off_chain = 0;
-	size_t off_tors_uv = 0, off_tors_mv = 0, off_tors_ends = 0, off_tor_items = 0, off_pairs = 0;
+	size_t off_tors_uv = 0, off_tors_mv = 0, off_tors_ends = 0, off_tor_items = 0, off_pairs2 = 0, off_gpairs = 0;
 	// cost model inputs (algorithmic work per evaluation)
 	long rot_ops = 0;     // torsion rotations + general rotations applied per pose
 };
