@@ -589,13 +589,16 @@ def _ligand_text(config_id, idx, n_heavy, n_tors, types=None):
 
 
 def run_batch(args):
-    """--mode batch: uneven ligands docked by the batch engine (all ligands and
-    runs admitted at once, one persistent launch) next to plain
-    per-ligand dockings through the reference kernel API, same ligands, same
-    budget.  A bounded sample of the batching configuration (1024 ligands,
-    10-64 heavy atoms, 0-32 torsions, nrun 20, 2.5M evals per run), or with
-    --batch-config 4 of the flexible-receptor one (80^3 maps, 7 types + e + d,
-    2 flexible residues of 8-10 atoms and 2-4 torsions, nrun 50, ADAM)."""
+    """--mode batch: ligands docked by the batch engine (all ligands and runs
+    admitted at once, one persistent launch) next to plain per-ligand
+    dockings through the reference kernel API, same ligands, same budget.
+    The batching configuration (--nlig 1024 --nev 2500000: 10-64 heavy atoms,
+    0-32 torsions, nrun 20, ADADELTA), or with --batch-config 4 the
+    flexible-receptor one (--nlig 256 --nev 2500000 --lsmet adam: 80^3 maps,
+    7 types + e + d, 2 flexible residues of 8-10 atoms and 2-4 torsions,
+    ligands of 40 heavy atoms / 10 torsions, nrun 50); smaller --nlig / --nev
+    give bounded samples of either.  The plain arms dock --plain-sample of the
+    ligands one at a time and scale their time to the whole set by cost."""
     import torch
     from adgpu_b200 import device, dock, engine, frontend, synth
     w = WORKLOAD
@@ -605,7 +608,9 @@ def run_batch(args):
     grid = frontend.Grid.from_maps(synth.quantize_maps(synth.make_maps_fast(spec)), types, spec.spacing, spec.origin)
     rng = np.random.default_rng(3)
     nlig, nrun, nev = args.nlig, (50 if cfg4 else 20), args.nev
-    sizes = [(int(rng.integers(10, 65)), int(rng.integers(0, 33))) for _ in range(nlig)]
+    # cfg3: heavy atoms uniform in 10-64, torsions in 0-32; cfg4: ligands as
+    # the plain configuration's (40 heavy atoms, 10 torsions), one seed each
+    sizes = [(40, 10) if cfg4 else (int(rng.integers(10, 65)), int(rng.integers(0, 33))) for _ in range(nlig)]
     run = frontend.default_dockpars(grid.spacing, 150)
     flex = None
     ltypes = None
@@ -621,6 +626,8 @@ def run_batch(args):
     en = engine.Engine(threads_per_pose=args.engine_tpp)
     rec = en.add_receptor(grid)
     torch.cuda.synchronize()
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
     t0 = time.perf_counter()
     ids = [en.submit(lg, rec, args.lsmet, max_evals=nev) for lg in ligs]
     tpps = {}
@@ -630,6 +637,7 @@ def run_batch(args):
     en.run()
     res = [en.result(i) for i in ids]
     t_batch = time.perf_counter() - t0
+    clocks = sampler.stop()
     ev_batch = sum(int(r.evals.sum()) for r in res)
     st = en.stats()
     util = st.worker_busy_s / st.worker_span_s if st.worker_span_s > 0 else None
@@ -666,7 +674,7 @@ def run_batch(args):
                         "worker_utilisation": util, "tasks": int(st.tasks)},
             "plain": plain,
             "batched_over_plain_ligands_per_hour": {k: lph_b / v["ligands_per_hour"] for k, v in plain.items()},
-            "tpp_classes": tpps}
+            "tpp_classes": tpps, "clocks_batched": clocks}
 
 
 def run_serve(args):
@@ -710,6 +718,8 @@ def run_serve(args):
                        threads_per_pose=args.engine_tpp)
     recs = [en.add_receptor(g) for g in grids]
     # serving loop
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
     t_start = time.perf_counter()
     pending, live, lat, queued = list(range(nreq)), {}, [], []
     done_n = 0
@@ -744,17 +754,19 @@ def run_serve(args):
             time.sleep(0.001)
     t_total = time.perf_counter() - t_start
     torch.cuda.synchronize()
+    clocks = sampler.stop()
     lat = np.array(lat)
     return {"mode": "serve", "requests": nreq, "nrun": nrun, "nev_per_run": nev, "receptors": "60^3, 80^3, 100^3",
             "batched_capacity_ligands_per_s": capacity, "arrival_rate_per_s": rate,
             "ligands_per_hour": 3600.0 * nreq / t_total, "latency_p50_s": float(np.percentile(lat, 50)),
-            "latency_p99_s": float(np.percentile(lat, 99)), "memory_budget_gb": args.budget_gb,
+            "latency_p99_s": float(np.percentile(lat, 99)), "latency_p90_s": float(np.percentile(lat, 90)),
+            "latency_mean_s": float(lat.mean()), "latency_max_s": float(lat.max()), "memory_budget_gb": args.budget_gb,
             "gens_per_tick": args.gens_per_tick, "tick_ms": args.tick_ms, "ticks": int(en.stats().ticks),
             "results_processed_on_device": bool(args.process_results), "threads_per_pose": {0: 32, -1: "tuned"}.get(args.engine_tpp, args.engine_tpp),
             "host_seconds": {"submit": t_submit, "tick": t_tick, "results": t_result, "total": t_total,
                              "engine_kernels": en.stats().kernel_s},
             "worker_utilisation": (en.stats().worker_busy_s / en.stats().worker_span_s
-                                   if en.stats().worker_span_s > 0 else None)}
+                                   if en.stats().worker_span_s > 0 else None), "clocks": clocks}
 
 
 def run_result(args):

@@ -153,3 +153,18 @@ def gradient_bound(case: Case, ref: np.ndarray) -> np.ndarray:
     bound = scale * n_terms / 1024.0
     bound[3:6] *= 1e3 / 1024.0 * 8.0
     return 1e-4 * np.abs(ref[..., :ng]) + bound
+
+
+def generic_pairs(case: Case) -> int:
+    """Intramolecular pairs whose vdW exponents are not the AD4 force field's
+    12-6 / 12-10 (modified pair potentials)."""
+    kin = abi.KcIntra.from_buffer_copy(bytes(case.tables["intra"]))
+    ii = abi.KcInterintra.from_buffer_copy(bytes(case.tables["interintra"]))
+    dp = case.dockpars
+    nat, q = dp.num_of_atypes, dp.num_of_intraE_contributors
+    ex = np.array(kin.VWpars_exp_const[:nat * nat], np.int64).reshape(nat, nat)
+    pairs = np.frombuffer(bytes(case.tables["intracontrib"]), np.uint32)[:2 * q].reshape(-1, 2)
+    t = np.array(ii.atom_types_const[:dp.num_of_atoms], np.int64)
+    e = ex[t[pairs[:, 0]], t[pairs[:, 1]]]
+    m, n = (e >> 8) & 0xFF, e & 0xFF
+    return int(((m != 12) | ((n != 6) & (n != 10))).sum())

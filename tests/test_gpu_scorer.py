@@ -122,3 +122,28 @@ def test_per_term_energies(cases, name):
     # the terms add up to the energy (plus the out-of-grid penalties)
     total = t[:, :7].astype(np.float64).sum(axis=1) + 16777216.0 * t[:, 7]
     assert np.allclose(total, e, rtol=1e-5, atol=1e-3)
+
+
+@pytest.mark.parametrize("tpp", [32, 64])
+def test_modified_pair_exponents(tmp_path, tpp, monkeypatch):
+    """Modified vdW pair potentials (the reference's --modpair: C-C as 13-7,
+    C-A as 12-8) are scored by the general-exponent pair loop next to the AD4
+    pairs: energies, gradients and the per-term split by the same rules as
+    the AD4 pairs."""
+    from adgpu_b200 import device
+    monkeypatch.setenv("ADGPU_THREADS_PER_POSE", str(tpp))
+    case = helpers.make_case(str(tmp_path / "mod"), 40, ["C", "A", "N", "OA", "HD"], 16, 4, 2, config_id=1,
+                             extra_args=("--modpair", "C:C,4.00,0.150,13,7/C:A,4.00,0.150,12,8"))
+    assert helpers.generic_pairs(case) > 20
+    dj = _activate(case)
+    g = helpers.in_box_genotypes(case, 1000, seed=11)
+    e_gpu, gr_gpu = device.score(g, True)
+    e_ref, gr_ref = case.host.score(g, True, nthreads=8)
+    assert np.all(np.abs(e_gpu - e_ref) <= helpers.energy_tolerance(e_ref)), np.abs(e_gpu - e_ref).max()
+    ng = case.ngenes
+    assert np.all(np.abs(gr_gpu[:, :ng] - gr_ref[:, :ng]) <= helpers.gradient_bound(case, gr_ref))
+    e, t = device.score_terms(g[:200])
+    ref = np.array([case.host.score_terms(x)[2] for x in g[:200]])
+    scale = np.abs(ref[:, :7]).sum(axis=1, keepdims=True)
+    assert np.all(np.abs(t[:, :7] - ref[:, :7]) <= 1e-4 * np.abs(ref[:, :7]) + 1e-6 * scale + 1e-5)
+    del dj
