@@ -15,7 +15,7 @@ LSMET = {"sw": 0, "ad": 1, "adam": 2, "fire": 3}
 class EngineConfig(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_size_t), ("threads_per_pose", C.c_int),
                 ("gens_per_tick", C.c_int), ("device", C.c_int), ("tick_ms", C.c_float),
-                ("idle_timeout_ms", C.c_float)]
+                ("idle_timeout_ms", C.c_float), ("priority", C.c_int)]
 
 
 class RequestParams(C.Structure):
@@ -72,8 +72,9 @@ class Result:
 
 class Engine:
     def __init__(self, memory_budget_bytes: int = 0, threads_per_pose: int = 0, gens_per_tick: int = 0,
-                 device: int = 0, tick_ms: float = 0.0, idle_timeout_ms: float = 0.0):
-        cfg = EngineConfig(memory_budget_bytes, threads_per_pose, gens_per_tick, device, tick_ms, idle_timeout_ms)
+                 device: int = 0, tick_ms: float = 0.0, idle_timeout_ms: float = 0.0, priority: int = 0):
+        cfg = EngineConfig(memory_budget_bytes, threads_per_pose, gens_per_tick, device, tick_ms, idle_timeout_ms,
+                           priority)
         h = C.c_void_p()
         lib.check(_L().adgpu_engine_create(C.byref(cfg), C.byref(h)), "engine_create")
         self.h = h

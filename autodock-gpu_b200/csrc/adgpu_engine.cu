@@ -103,6 +103,7 @@ struct TickArgs {
 	const RunRef* work;
 	TickRun* runs;              // per work item
 	uint8_t* work_done;         // per work item: run finished (written when it retires)
+	const uint32_t* prio;       // per work item: its request's rank by age (0 oldest), or null: all equal
 	long long tick_ns;          // > 0: a worker takes no new task once this long after it started
 	long long idle_ns;          // a worker that finds no task for this long stops and reports an error
 	TickClass cls[3];           // threads per pose 32, 64, 128
@@ -142,7 +143,9 @@ __device__ bool take_task(const TickArgs& t, const TickClass& C, int lane, int w
 	unsigned int rot = (unsigned int)worker * 2654435761u;
 	for (int spins = 0; spins < (1 << 30); spins++) {
 		if (H.deadline && global_ns() > H.deadline) return false;
-		// the run served last, then a scan for the least advanced run with entities left
+		// the run served last, then a scan for the run with entities left that
+		// has the lowest (request rank, step): with ranks, the oldest request's
+		// least advanced run; without, the least advanced run
 		int cand = -1;
 		if (spins == 0 && H.sticky >= 0) {
 			cand = H.sticky;
@@ -158,7 +161,9 @@ __device__ bool take_task(const TickArgs& t, const TickClass& C, int lane, int w
 				const unsigned int taken = (unsigned int)r.x, phase = (unsigned int)r.y;
 				const int step = (int)(phase >> 1);
 				if (taken < (unsigned int)r.z && step < r.w) {
-					const unsigned long long key = ((unsigned long long)(unsigned int)step << 32) |
+					const unsigned int rank = t.prio ? t.prio[w] : 0u;
+					const unsigned long long key = ((unsigned long long)rank << 48) |
+					                               ((unsigned long long)min(step, 0xFFFF) << 32) |
 					                               (((unsigned int)w - (unsigned int)C.w0 + rot) % (unsigned int)C.nw);
 					best = key < best ? key : best;
 				}
@@ -512,6 +517,7 @@ struct Engine {
 	// counters and done flags; the classes' control blocks
 	RunRef* d_work = nullptr; int d_work_cap = 0;
 	TickRun* d_runs = nullptr;
+	uint32_t* d_prio = nullptr;   // per work item: request rank (priority 1)
 	uint8_t* d_done = nullptr;
 	QueueCtl* d_ctl = nullptr;
 	long long idle_ns = kIdleNs;                  // a pose group's idle limit (engine configuration)
@@ -619,6 +625,10 @@ adgpu_status adgpu_engine_create(const adgpu_engine_config* cfg, adgpu_engine** 
 	    E.cfg.threads_per_pose != 64 && E.cfg.threads_per_pose != 128) {
 		delete en;
 		return fail(ADGPU_ERR_ARG, "threads_per_pose must be -1, 0, 32, 64 or 128");
+	}
+	if (E.cfg.priority != 0 && E.cfg.priority != 1) {
+		delete en;
+		return fail(ADGPU_ERR_ARG, "priority must be 0 or 1");
 	}
 	cudaError_t e = cudaSetDevice(E.cfg.device);
 	if (e != cudaSuccess) { delete en; return cuda_fail(e, "set device"); }
@@ -798,6 +808,7 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	int max_atoms[NC], max_tors[NC], max_tasks[NC];
 	double weight[NC];
 	for (int c = 0; c < NC; c++) { max_atoms[c] = 1; max_tors[c] = 0; max_tasks[c] = 1; weight[c] = 0; }
+	std::vector<uint32_t> wprio[NC];      // request rank by age (E.requests is ordered by id = admission)
 	for (auto& kv : E.requests) {
 		Request& r = *kv.second;
 		if (r.done) continue;
@@ -805,7 +816,10 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 		const int idx = (int)reqs.size();
 		reqs.push_back(r.dev);
 		order.push_back(&r);
-		for (int k = 0; k < r.runs; k++) work[cls].push_back({idx, k});
+		for (int k = 0; k < r.runs; k++) {
+			work[cls].push_back({idx, k});
+			wprio[cls].push_back((uint32_t)std::min(idx, 0xFFFF));
+		}
 		const adgpu_dockpars& dp = r.dev.a.dp;
 		max_atoms[cls] = std::max(max_atoms[cls], r.natoms);
 		max_tors[cls] = std::max(max_tors[cls], r.ntors);
@@ -816,9 +830,11 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	if (reqs.empty()) return ADGPU_OK;
 	size_t start[NC];
 	std::vector<RunRef> all;
+	std::vector<uint32_t> all_prio;
 	for (int c = 0; c < NC; c++) {
 		start[c] = all.size();
 		all.insert(all.end(), work[c].begin(), work[c].end());
+		all_prio.insert(all_prio.end(), wprio[c].begin(), wprio[c].end());
 	}
 	const size_t nwork = all.size();
 	if (nwork >= (size_t)0x3fffffff) return fail(ADGPU_ERR_LIMIT, "too many runs admitted at once");
@@ -832,13 +848,14 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	if ((int)nwork > E.d_work_cap) {
 		if (E.d_work) cudaFree(E.d_work);
 		E.d_work_cap = std::max<int>((int)nwork * 2, 256);
-		const size_t per = sizeof(RunRef) + sizeof(TickRun) + 1;
+		const size_t per = sizeof(RunRef) + sizeof(TickRun) + 1 + sizeof(uint32_t);
 		e = cudaMalloc(&E.d_work, per * E.d_work_cap + 256);
 		if (e != cudaSuccess) { E.d_work = nullptr; E.d_work_cap = 0; return cuda_fail(e, "work list"); }
 		char* B = reinterpret_cast<char*>(E.d_work) + sizeof(RunRef) * E.d_work_cap;
 		B = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(B) + 15) & ~uintptr_t(15));
 		E.d_runs = reinterpret_cast<TickRun*>(B);
-		E.d_done = reinterpret_cast<uint8_t*>(E.d_runs + E.d_work_cap);
+		E.d_prio = reinterpret_cast<uint32_t*>(E.d_runs + E.d_work_cap);
+		E.d_done = reinterpret_cast<uint8_t*>(E.d_prio + E.d_work_cap);
 	}
 	QueueCtl h_ctl[NC];
 	memset(h_ctl, 0, sizeof(h_ctl));
@@ -851,6 +868,8 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 	cb.start[NC] = (int)nwork;
 	e = cudaMemcpyAsync(E.d_reqs, reqs.data(), sizeof(ReqDev) * reqs.size(), cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_work, all.data(), sizeof(RunRef) * nwork, cudaMemcpyHostToDevice, E.stream);
+	if (e == cudaSuccess && E.cfg.priority == 1)
+		e = cudaMemcpyAsync(E.d_prio, all_prio.data(), sizeof(uint32_t) * nwork, cudaMemcpyHostToDevice, E.stream);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(E.d_ctl, h_ctl, sizeof(h_ctl), cudaMemcpyHostToDevice, E.stream);
 	if (e != cudaSuccess) return cuda_fail(e, "tick upload");
 	const int lgrid = (int)std::min<size_t>((nwork + 255) / 256, 1024);
@@ -867,6 +886,7 @@ adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 		TickArgs t;
 		memset(&t, 0, sizeof(t));
 		t.reqs = E.d_reqs; t.work = E.d_work; t.runs = E.d_runs; t.work_done = E.d_done;
+		t.prio = E.cfg.priority == 1 ? E.d_prio : nullptr;
 		t.tick_ns = (long long)(1e6 * (double)E.cfg.tick_ms);
 		t.idle_ns = E.idle_ns;
 		for (int k = 0; k < 3; k++) {

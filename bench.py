@@ -517,8 +517,8 @@ def run_engine(args, rank, world, local_rank):
             sv = run_serve(sargs)
             line["serving"] = {k: sv[k] for k in ("requests", "nrun", "nev_per_run", "receptors",
                                                   "batched_capacity_ligands_per_s", "arrival_rate_per_s",
-                                                  "ligands_per_hour", "latency_p50_s", "latency_p99_s", "tick_ms",
-                                                  "results_processed_on_device")}
+                                                  "ligands_per_hour", "latency_p50_s", "latency_p90_s", "latency_p99_s",
+                                                  "tick_ms", "threads_per_pose", "priority", "results_processed_on_device")}
         if not args.no_result:
             rr = run_result(args)
             line["result_processing"] = {k: rr[k] for k in ("workload", "gpu_ms_all_entities", "reference_host_ms",
@@ -700,9 +700,15 @@ def run_serve(args):
                             seed=w["seed"], num_runs=nrun) for i, t in enumerate(targets)]
     budget = args.budget_gb << 30
     natoms = [lg.dockpars.num_of_atoms for lg in ligs]
-    # capacity: a batch of requests run to completion in one launch
+    # 64 threads per pose unless asked otherwise: a request's latency is the
+    # chain of its runs' generations, each ending with its longest local
+    # search, which two warps per pose shorten (p50 0.96 s against 1.27 s at
+    # 80 % load for 4 % less capacity)
+    tpp = args.engine_tpp if args.engine_tpp else 64
+    # capacity: a batch of requests run to completion in one launch, by an
+    # engine with the serving engine's settings
     cap_n = min(nreq, 48)
-    cap = engine.Engine(memory_budget_bytes=budget)
+    cap = engine.Engine(memory_budget_bytes=budget, threads_per_pose=tpp, priority=args.priority)
     crecs = [cap.add_receptor(g) for g in grids]
     t0 = time.perf_counter()
     ids = [cap.submit(ligs[i], crecs[targets[i]], args.lsmet, max_evals=nev) for i in range(cap_n)]
@@ -715,7 +721,7 @@ def run_serve(args):
     arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
     # the serving engine: ticks end on a wall-clock deadline (or a generation count)
     en = engine.Engine(memory_budget_bytes=budget, gens_per_tick=args.gens_per_tick, tick_ms=args.tick_ms,
-                       threads_per_pose=args.engine_tpp)
+                       threads_per_pose=tpp, priority=args.priority)
     recs = [en.add_receptor(g) for g in grids]
     # serving loop
     sampler = ClockSampler(torch.cuda.current_device())
@@ -762,7 +768,8 @@ def run_serve(args):
             "latency_p99_s": float(np.percentile(lat, 99)), "latency_p90_s": float(np.percentile(lat, 90)),
             "latency_mean_s": float(lat.mean()), "latency_max_s": float(lat.max()), "memory_budget_gb": args.budget_gb,
             "gens_per_tick": args.gens_per_tick, "tick_ms": args.tick_ms, "ticks": int(en.stats().ticks),
-            "results_processed_on_device": bool(args.process_results), "threads_per_pose": {0: 32, -1: "tuned"}.get(args.engine_tpp, args.engine_tpp),
+            "priority": {0: "least advanced run", 1: "oldest request"}[args.priority],
+            "results_processed_on_device": bool(args.process_results), "threads_per_pose": {-1: "tuned"}.get(tpp, tpp),
             "host_seconds": {"submit": t_submit, "tick": t_tick, "results": t_result, "total": t_total,
                              "engine_kernels": en.stats().kernel_s},
             "worker_utilisation": (en.stats().worker_busy_s / en.stats().worker_span_s
@@ -868,8 +875,8 @@ def main():
     ap.add_argument("--nrun", type=int, default=0, help="runs per ligand (ls-kernel / loop-kernel modes)")
     ap.add_argument("--tpp", type=int, default=32, help="threads per pose of the measured launches (ls-kernel mode)")
     ap.add_argument("--engine-tpp", type=int, default=0,
-                    help="engine threads per pose (batch / serve modes): 0 = the engine's default (32), "
-                         "-1 = tuned per ligand size, or 32, 64, 128")
+                    help="engine threads per pose (batch / serve modes): 0 = the mode's default (batch: the "
+                         "engine's, 32; serve: 64), -1 = tuned per ligand size, or 32, 64, 128")
     ap.add_argument("--nlig", type=int, default=64, help="ligands (batch mode)")
     ap.add_argument("--batch-config", type=int, default=3, choices=[3, 4],
                     help="batch mode workload: 3 (uneven ligands) or 4 (80^3 maps, 2 flexible residues, nrun 50)")
@@ -883,6 +890,8 @@ def main():
     ap.add_argument("--rate", type=float, default=0.0,
                     help="request arrival rate per second (serve mode; 0: 80%% of the measured capacity)")
     ap.add_argument("--tick-ms", type=float, default=50.0, help="wall-clock length of an engine tick (serve mode; 0: none)")
+    ap.add_argument("--priority", type=int, default=1, choices=[0, 1],
+                    help="serve mode: runs served first, 0 the least advanced, 1 the oldest request's")
     args = ap.parse_args()
     if args.mode == "ls-kernel":
         run_kernel_only(args)

@@ -461,7 +461,8 @@ adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_ref
  * advances every admitted run by up to gens_per_tick generations, or until
  * tick_ms has passed, in one persistent launch per local-search method whose
  * pose groups take tasks (one entity of a run's generation: its GA step and
- * its local search) from the runs' own counters, least advanced run first;
+ * its local search) from the runs' own counters, least advanced run first
+ * (or, with priority 1, the oldest request's runs first);
  * between ticks requests can be submitted and results taken (continuous
  * batching).  Each run stops on its own budget (evals >=
  * max_evals or generations >= max_gens), so a request's result does not
@@ -477,6 +478,10 @@ typedef struct {
 	float  tick_ms;              /* > 0: a tick also ends after this long: no pose group takes a new task after it */
 	float  idle_timeout_ms;      /* a pose group that finds no task for this long while runs are active ends
 	                                the tick with ADGPU_ERR_TIMEOUT; 0: 2000 */
+	int    priority;             /* which run a free pose group serves: 0 the least advanced run (a batch
+	                                finishes together); 1 a run of the oldest admitted request, least
+	                                advanced first among its runs (a stream: requests finish in order,
+	                                lower latency); results are the same either way */
 } adgpu_engine_config;
 
 typedef struct {

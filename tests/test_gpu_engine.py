@@ -184,10 +184,12 @@ def test_ga_only_and_mixed_population_sizes(grid, monkeypatch):
             assert int(r.evals[0]) == pop * (gens + 1) - gens    # GA only: P per generation minus the elite
 
 
-def test_time_sliced_ticks_give_the_same_results(grid):
+@pytest.mark.parametrize("priority", [0, 1])
+def test_time_sliced_ticks_give_the_same_results(grid, priority):
     """Ticks that end on a wall-clock deadline (tick_ms) instead of a
     generation count cut runs at arbitrary generations; results must not
-    depend on where the cuts fall."""
+    depend on where the cuts fall, nor on which runs the pose groups serve
+    first (priority 1: the oldest request's runs)."""
     ligs = [ligand(grid, 30 + i, 16 + 4 * i, 3 + i, runs=2) for i in range(3)]
     nev = 30_000
     ref = []
@@ -198,7 +200,7 @@ def test_time_sliced_ticks_give_the_same_results(grid):
         en.run()
         ref.append(en.result(rid))
         en.close()
-    en = engine.Engine(threads_per_pose=32, tick_ms=2.0)
+    en = engine.Engine(threads_per_pose=32, tick_ms=2.0, priority=priority)
     rec = en.add_receptor(grid)
     ids = [en.submit(lg, rec, "ad", max_evals=nev) for lg in ligs]
     ticks = 0
