@@ -12,6 +12,7 @@
 #include "adgpu_autostop.cuh"
 #include "adgpu_tables.h"
 #include "adgpu_pipeline.h"
+#include "adgpu_nvtx.h"
 
 #ifndef ADGPU_MIN_CTAS
 #define ADGPU_MIN_CTAS 6     // 6 CTAs x 4 warps per SM: <= 80 registers, no spills
@@ -551,6 +552,7 @@ adgpu_status adgpu_dock_resident(int lsmet, uint32_t num_runs, uint64_t max_eval
                                  float* c1, float* e1, float* c2, float* e2,
                                  int* final_is_second, uint32_t* generations)
 {
+	adgpu::NvtxRange nvtx_range("adgpu_dock_resident");
 	ApiState& s = api();
 	if (!s.ready) return fail(ADGPU_ERR_NOT_READY, "adgpu_set_kernels_gpu_data not called");
 	if (lsmet < 0 || lsmet > 3) return fail(ADGPU_ERR_ARG, "lsmet must be 0 (sw), 1 (ad), 2 (adam) or 3 (fire)");
@@ -565,6 +567,7 @@ adgpu_status adgpu_dock_resident_autostop(int lsmet, uint32_t num_runs, uint64_t
                                           float* c1, float* e1, float* c2, float* e2,
                                           int* final_is_second, uint32_t* generations, int* autostopped)
 {
+	adgpu::NvtxRange nvtx_range("adgpu_dock_resident_autostop");
 	ApiState& s = api();
 	if (!s.ready) return fail(ADGPU_ERR_NOT_READY, "adgpu_set_kernels_gpu_data not called");
 	if (lsmet < 0 || lsmet > 3) return fail(ADGPU_ERR_ARG, "lsmet must be 0 (sw), 1 (ad), 2 (adam) or 3 (fire)");

@@ -32,6 +32,7 @@
 #include "adgpu_prep.h"
 #include "adgpu_result.h"
 #include "adgpu_tables.h"
+#include "adgpu_nvtx.h"
 
 namespace adgpu {
 
@@ -692,6 +693,7 @@ adgpu_status adgpu_engine_add_receptor(adgpu_engine* en, const adgpu_grid* grid,
 
 adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, const adgpu_request_params* rp, uint64_t* request_id)
 {
+	adgpu::NvtxRange nvtx_range("adgpu_engine_submit");
 	if (!en || !lig || !rp || !request_id) return fail(ADGPU_ERR_ARG, "null argument");
 	Engine& E = en->e;
 	std::lock_guard<std::mutex> lk(E.mu);
@@ -797,6 +799,7 @@ adgpu_status adgpu_engine_submit(adgpu_engine* en, const adgpu_ligand* lig, cons
 
 adgpu_status adgpu_engine_tick(adgpu_engine* en, int* completed)
 {
+	adgpu::NvtxRange nvtx_range("adgpu_engine_tick");
 	if (!en) return fail(ADGPU_ERR_ARG, "null engine");
 	Engine& E = en->e;
 	std::lock_guard<std::mutex> lk(E.mu);
@@ -1043,6 +1046,7 @@ adgpu_status adgpu_engine_process_result(adgpu_engine* en, uint64_t request_id, 
                                          double* best_xyz, float* peratom, float* entities, float* final_population,
                                          float* final_energies)
 {
+	adgpu::NvtxRange nvtx_range("adgpu_engine_process_result");
 	if (!en || !params) return fail(ADGPU_ERR_ARG, "null argument");
 	Engine& E = en->e;
 	std::lock_guard<std::mutex> lk(E.mu);

@@ -19,6 +19,7 @@
 #include "adgpu_prep.h"
 #include "adgpu_result.h"
 #include "adgpu_tables.h"
+#include "adgpu_nvtx.h"
 
 namespace adgpu {
 namespace {
@@ -700,6 +701,7 @@ adgpu_status adgpu_process_result(const adgpu_ligand* lig, const float* grid_ref
                                   adgpu_run_result* runs_out, adgpu_cluster* clusters_out, int* num_clusters,
                                   double* best_xyz, float* peratom, float* entities)
 {
+	adgpu::NvtxRange nvtx_range("adgpu_process_result");
 	if (!lig) return fail(ADGPU_ERR_ARG, "null argument");
 	// a blocking stream: ordered after the caller's work on the legacy
 	// default stream (where the kernel API and torch's default stream write
