@@ -497,6 +497,7 @@ def run_engine(args, rank, world, local_rank):
                                   "steps": len(t_o), "generations_per_docking": g_o // len(t_o),
                                   "ligands_per_hour": 3600.0 * len(t_o) / sum(t_o), "docking_loop": dock.last_stats()}
         del job_o, bufs_o
+        line["cfg1_gpu"] = gpu_cfg1(dev)
         job.activate()
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.lsmet)
@@ -508,7 +509,8 @@ def run_engine(args, rank, world, local_rank):
             # the batching comparison on a bounded sample of its configuration
             bvp = run_batch(args)
             line["batched_vs_plain"] = {k: bvp[k] for k in ("ligands", "nrun", "nev_per_run", "heavy_atoms", "batched",
-                                                            "plain", "batched_over_plain_ligands_per_hour", "tpp_classes")}
+                                                            "plain", "batched_over_plain_ligands_per_hour", "tpp_classes",
+                                                            "clocks_batched")}
         if not args.no_serve:
             # the serving loop on a shorter request stream (same settings as --mode serve)
             sargs = argparse.Namespace(**vars(args))
@@ -518,13 +520,50 @@ def run_engine(args, rank, world, local_rank):
             line["serving"] = {k: sv[k] for k in ("requests", "nrun", "nev_per_run", "receptors",
                                                   "batched_capacity_ligands_per_s", "arrival_rate_per_s",
                                                   "ligands_per_hour", "latency_p50_s", "latency_p90_s", "latency_p99_s",
-                                                  "tick_ms", "threads_per_pose", "priority", "results_processed_on_device")}
+                                                  "tick_ms", "threads_per_pose", "priority", "results_processed_on_device",
+                                                  "clocks")}
         if not args.no_result:
             rr = run_result(args)
             line["result_processing"] = {k: rr[k] for k in ("workload", "gpu_ms_all_entities", "reference_host_ms",
                                                             "speedup_vs_reference", "clusters", "parity")}
         del evals_per_docking
     return line
+
+
+def gpu_cfg1(dev, steps: int = 3):
+    """The small CPU-runnable configuration docked on the GPU: 40^3 maps,
+    16 heavy atoms / 4 torsions, nrun 10, pop 150, 2.5M evaluations per run,
+    ADADELTA (the docking the CPU baseline times completely)."""
+    import torch
+    from adgpu_b200 import device, dock, frontend, synth
+    w = WORKLOAD
+    spec = synth.grid_spec(40, w["types"], seed=12345 + 1)
+    grid = frontend.Grid.from_maps(synth.quantize_maps(synth.make_maps(spec)), w["types"], spec.spacing, spec.origin)
+    text = "\n".join(synth.pdbqt_lines(synth.ligand_for(1, 0, 16, 4))[0]) + "\n"
+    lig = frontend.Ligand(grid, text, None, run=frontend.default_dockpars(grid.spacing, w["pop"]), seed=w["seed"],
+                          num_runs=10)
+    job = device.DeviceJob(lig.tables, lig.dockpars, grid.reference_layout(), 10, lig.prng, device=dev)
+    job.activate()
+    bufs = (*job.population(), *job.population())
+    init_dev = torch.from_numpy(lig.initpop).to(dev)
+    prng0 = job.prng.clone()
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ts, ev, gens = [], 0, 0
+    for i in range(steps + 1):
+        job.prng.copy_(prng0)
+        torch.cuda.synchronize()
+        ea.record()
+        r = dock.dock(job, init_dev, "ad", w["nev"], 42000, buffers=bufs)
+        eb.record()
+        torch.cuda.synchronize()
+        if i:
+            ts.append(ea.elapsed_time(eb) / 1e3)
+            ev += int(r.evals_per_run.sum())
+            gens = r.generations
+    return {"workload": "40^3 maps, 16 heavy atoms / 4 torsions, nrun 10, pop 150, nev 2.5M, lsmet ad",
+            "seconds_per_docking": sum(ts) / len(ts), "evals_per_s": ev / sum(ts), "generations": gens,
+            "ligands_per_hour": 3600.0 * len(ts) / sum(ts), "best_energy": float(r.energies.min().item()),
+            "docking_loop": dock.last_stats()}
 
 
 def run_kernel_only(args):

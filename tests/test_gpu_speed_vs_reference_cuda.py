@@ -1,8 +1,11 @@
 """Throughput against the reference's own CUDA kernels (cuda/*.cu compiled
 unchanged for sm_100a with the reference's flags, oracle/_ref) on the same
 GPU: the cfg2 ligand (40 heavy atoms, 10 torsions), 100 runs x 150
-entities, the same GpuData and population.  Prints one JSON line with both
-rates; fails if the engine's kernels are slower than the reference's."""
+entities, the same GpuData and population: the ADADELTA local search, the GA
+generation and the scorer launch by launch, and a whole docking (500k
+evaluations per run) through each side's own generation loop.  Prints one
+JSON line with both rates; fails if the engine is slower than the reference
+in any of the local search, the GA or the docking."""
 import ctypes as C
 import json
 import os
@@ -76,6 +79,44 @@ def test_kernels_faster_than_reference_cuda(case):
         call()
         dt = _timed(call)
         out[f"score_grad_{name}_evals_per_s"] = len(g) / dt
+    # a whole docking of the same ligand (100 runs, 500k evaluations per run,
+    # ADADELTA): the reference's generation loop over its own kernels, one
+    # synchronous call per kernel per generation (docking_with_gpu,
+    # host/src/performdocking.cpp.Cuda:684-831), against adgpu_dock_resident
+    nev = 500_000
+    for name in ("engine", "reference_cuda"):
+        job = device.DeviceJob(case.tables, dp, case.grid, R, case.prng)
+        cur, ecur = job.population(case.initpop)
+        nxt, enxt = job.population()
+        if name == "engine":
+            job.activate()
+            lib.call("adgpu_calc_initpop", R * P, T, cur, ecur)
+            lib.call("adgpu_sum_evals", R, T)
+        else:
+            refpy.cuda_lib().adgpu_refcuda_set_gpudata(C.cast(C.pointer(job.g), C.c_void_p))
+            refpy.cuda_call("calc_initpop", R * P, T, cur, ecur)
+            refpy.cuda_call("sum_evals", R, T)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        if name == "engine":
+            fin, gn = C.c_int(0), C.c_uint32(0)
+            lib.call("adgpu_dock_resident", 1, R, nev, 42000, cur, ecur, nxt, enxt, C.byref(fin), C.byref(gn))
+            gens = gn.value
+        else:
+            gens = 0
+            while job.evals_runs.sum().item() / R < nev:
+                refpy.cuda_call("gen_and_eval_newpops", R * P, T, cur, ecur, nxt, enxt)
+                refpy.cuda_call("gradient_minad", R * L, T, nxt, enxt)
+                refpy.cuda_call("sum_evals", R, T)
+                gens += 1
+                cur, nxt, ecur, enxt = nxt, cur, enxt, ecur
+        b.record()
+        torch.cuda.synchronize()
+        dt = a.elapsed_time(b) / 1e3
+        out[f"docking_{name}_s"] = dt
+        out[f"docking_{name}_evals_per_s"] = (int(job.evals_runs.sum().item()) - R * P) / dt
+        out[f"docking_{name}_generations"] = gens
     line = json.dumps(out)
     print(line)
     if os.environ.get("ADGPU_SPEED_OUT"):
@@ -83,3 +124,4 @@ def test_kernels_faster_than_reference_cuda(case):
             f.write(line + "\n")
     assert out["ls_ad_engine_evals_per_s"] > out["ls_ad_reference_cuda_evals_per_s"]
     assert out["ga_engine_entities_per_s"] > out["ga_reference_cuda_entities_per_s"]
+    assert out["docking_engine_evals_per_s"] > out["docking_reference_cuda_evals_per_s"]
