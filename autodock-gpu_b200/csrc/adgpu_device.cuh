@@ -121,6 +121,7 @@ struct LigDev {
 	// the AD4 pairs; ngpairs: pairs with other exponents)
 	int natoms, nlig, ngenes, ntors, npairs, ntoritems;
 	int npairs2, ngpairs;
+	int coupled;                 // 1: the two pairs of every record share their first atom
 	int map_e;                   // index of the e map in the cell record (0)
 	// grid
 	int gx, gy, gz;              // grid points per axis
@@ -378,6 +379,20 @@ __device__ __forceinline__ void pair_force(int* f3, uint32_t i, uint32_t j, floa
 	atomicAdd(fj, ix); atomicAdd(fj + 1, iy); atomicAdd(fj + 2, iz);
 }
 
+// The fixed-point forces of a couple (pairs A and B sharing atom c, second
+// atoms i and j): c's part of the two is summed in registers and added once.
+__device__ __forceinline__ void couple_force(int* f3, uint32_t c, uint32_t i, uint32_t j, float2 gx, float2 gy, float2 gz)
+{
+	const int ax = quant_scaled(gx.x), ay = quant_scaled(gy.x), az = quant_scaled(gz.x);
+	const int bx = quant_scaled(gx.y), by = quant_scaled(gy.y), bz = quant_scaled(gz.y);
+	int* fc = f3 + 3 * c;
+	int* fi = f3 + 3 * i;
+	int* fj = f3 + 3 * j;
+	atomicAdd(fc, -ax - bx); atomicAdd(fc + 1, -ay - by); atomicAdd(fc + 2, -az - bz);
+	atomicAdd(fi, ax); atomicAdd(fi + 1, ay); atomicAdd(fi + 2, az);
+	atomicAdd(fj, bx); atomicAdd(fj + 1, by); atomicAdd(fj + 2, bz);
+}
+
 // Energy of the AD4 pairs this thread takes (records rank, rank + TPP, ...),
 // with, for GRAD, their fixed-point forces added to S.f3.  The terms are the
 // reference's (cuda/calcMergeEneGra.cu:418-602) rewritten with one reciprocal
@@ -387,8 +402,10 @@ __device__ __forceinline__ void pair_force(int* f3, uint32_t i, uint32_t j, floa
 // [r - hs, r + hs], the elec_min_distance floor as a max (and a min on 1/r).
 // TERMS (energy only): also adds this thread's vdW/H-bond, electrostatic,
 // desolvation and CG-G0 sums to tsum[0..3].
-template <int TPP, bool GRAD, bool TERMS = false>
-__device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, int rank, float* tsum = nullptr)
+// With COUPLED (the host's tables, L.coupled) the two pairs of a record share
+// their first atom: one position load and one set of atomics for it.
+template <int TPP, bool GRAD, bool TERMS, bool COUPLED>
+__device__ __forceinline__ float pair_loop(const LigDev& L, const PoseSmem& S, int rank, float* tsum)
 {
 	// loop invariants read once: when L lives in shared memory (the engine's
 	// per-task arguments) the force atomics below would otherwise force a
@@ -407,8 +424,9 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 	for (int d = rank; d < nrec; d += TPP, pr += (TPP / 32) * 128) {
 		const float4 q0 = __ldg(pr), q1 = __ldg(pr + 32), q2 = __ldg(pr + 64), q3 = __ldg(pr + 96);
 		const uint32_t ija = __float_as_uint(q3.z), ijb = __float_as_uint(q3.w);
-		const uint32_t a1 = ija & 0xFFu, a2 = ija >> 8, b1 = ijb & 0xFFu, b2 = ijb >> 8;
-		const float4 pa1 = xyz[a1], pa2 = xyz[a2], pb1 = xyz[b1], pb2 = xyz[b2];
+		const uint32_t a1 = ija & 0xFFu, a2 = ija >> 8, b1 = COUPLED ? a1 : (ijb & 0xFFu), b2 = ijb >> 8;
+		const float4 pa1 = xyz[a1], pa2 = xyz[a2], pb2 = xyz[b2];
+		const float4 pb1 = COUPLED ? pa1 : xyz[b1];
 		const float2 sx = f2(pa1.x - pa2.x, pb1.x - pb2.x);
 		const float2 sy = f2(pa1.y - pa2.y, pb1.y - pb2.y);
 		const float2 sz = f2(pa1.z - pa2.z, pb1.z - pb2.z);
@@ -473,8 +491,12 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 			// the same rounding as quant(sub * gdd))
 			const float2 gdd = f2mul(pg, f2mul(inv_dist, f2s(-kTermScale)));
 			const float2 gx = f2mul(sx, gdd), gy = f2mul(sy, gdd), gz = f2mul(sz, gdd);
-			pair_force(f3, a1, a2, gx.x, gy.x, gz.x);
-			pair_force(f3, b1, b2, gx.y, gy.y, gz.y);
+			if constexpr (COUPLED) {
+				couple_force(f3, a1, a2, b2, gx, gy, gz);
+			} else {
+				pair_force(f3, a1, a2, gx.x, gy.x, gz.x);
+				pair_force(f3, b1, b2, gx.y, gy.y, gz.y);
+			}
 		}
 	}
 	if constexpr (TERMS) {
@@ -484,6 +506,13 @@ __device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, 
 		tsum[3] += t_cg.x + t_cg.y;
 	}
 	return esum.x + esum.y;
+}
+
+template <int TPP, bool GRAD, bool TERMS = false>
+__device__ __forceinline__ float pair_terms(const LigDev& L, const PoseSmem& S, int rank, float* tsum = nullptr)
+{
+	return L.coupled ? pair_loop<TPP, GRAD, TERMS, true>(L, S, rank, tsum)
+	                 : pair_loop<TPP, GRAD, TERMS, false>(L, S, rank, tsum);
 }
 
 // Pairs with other exponents than 12-6 / 12-10 (modified pair potentials;

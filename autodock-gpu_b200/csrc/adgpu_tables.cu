@@ -28,61 +28,94 @@ size_t cell_grid_bytes(int gx, int gy, int gz, int num_map_atypes)
 	return (size_t)(gx - 1) * (gy - 1) * (gz - 1) * (size_t)(num_map_atypes + 2) * 8 * sizeof(float);
 }
 
-// Pair order for the scorer's force atomics.  One warp instruction handles an
-// aligned group of 32 consecutive pairs, and its atomics take one
-// shared-memory pass per pair that shares a bank (atom index mod 32) with
-// another pair of the group on the same side.  The pairs, sorted by the banks
-// of their atoms, are dealt round-robin over the groups, which spreads every
-// bank's pairs evenly; then each group flips pairs while that lowers the
-// larger bank count of its first-atom side plus that of its second-atom side.
-// A pair's energy and force do not depend on its orientation: the record
-// fields are computed from its original order and the force update is
-// antisymmetric (x1 - x2 = -(x2 - x1), symmetric fixed-point rounding), so
-// only the order of the per-thread energy sums changes.
-static void order_pairs(const uint32_t* pairs, int Q, std::vector<uint32_t>& pos, std::vector<uint8_t>& swapped)
+// Couples of pairs for the scorer's pair loop.  A thread takes two pairs per
+// step from one record: pair A, of an aligned group of 32 (one warp
+// instruction), and pair B, of the next group.  When both pairs share their
+// first atom, that atom's force from the two is summed in registers and added
+// with one set of shared-memory atomics instead of two, and its position is
+// loaded once.  Pairs are coupled at shared atoms: each atom, lowest degree
+// first, couples its still-uncoupled pairs two by two (a pair's orientation is
+// free: its terms do not depend on it and the force update is antisymmetric,
+// x1 - x2 = -(x2 - x1) with symmetric fixed-point rounding); a pair left over
+// gets an empty partner (both atoms the same, zero coefficients).
+struct Couple { uint32_t c; int a, b; };   // shared atom; pair indices (b < 0: empty)
+
+static uint32_t partner(const uint32_t* pairs, int p, uint32_t c)
 {
-	pos.assign(Q, 0);
-	swapped.assign(Q, 0);
-	if (Q == 0) return;
-	std::vector<int> idx(Q);
-	for (int p = 0; p < Q; p++) idx[p] = p;
-	std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
-		const uint32_t ka = ((pairs[2 * a] & 31) << 5) | (pairs[2 * a + 1] & 31);
-		const uint32_t kb = ((pairs[2 * b] & 31) << 5) | (pairs[2 * b + 1] & 31);
-		return ka < kb;
-	});
-	const int G = (Q + 31) / 32;
-	std::vector<std::vector<int>> groups(G);
+	return pairs[2 * p] == c ? pairs[2 * p + 1] : pairs[2 * p];
+}
+
+static void couple_pairs(const uint32_t* pairs, int Q, int N, std::vector<Couple>& out)
+{
+	out.clear();
+	std::vector<std::vector<int>> inc(N);
+	for (int p = 0; p < Q; p++) { inc[pairs[2 * p]].push_back(p); inc[pairs[2 * p + 1]].push_back(p); }
+	std::vector<int> order(N);
+	for (int v = 0; v < N; v++) order[v] = v;
+	std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return inc[x].size() < inc[y].size(); });
+	std::vector<uint8_t> used(Q, 0);
+	for (int v : order) {
+		int pending = -1;
+		for (int p : inc[v]) {
+			if (used[p]) continue;
+			if (pending < 0) { pending = p; continue; }
+			out.push_back({(uint32_t)v, pending, p});
+			used[pending] = used[p] = 1;
+			pending = -1;
+		}
+	}
+	for (int p = 0; p < Q; p++)
+		if (!used[p]) out.push_back({pairs[2 * p], p, -1});
+}
+
+// Slots of the couples: one record per couple, records in blocks of 32 (a
+// warp's step).  Couples sorted by the bank of their shared atom are dealt
+// round-robin over the blocks, which spreads every bank's couples evenly;
+// then within each block a couple swaps its A and B pairs while that lowers
+// the largest bank count of the A partners plus that of the B partners (the
+// shared atoms' atomics are one instruction per block, the partners' two).
+static void order_couples(const uint32_t* pairs, std::vector<Couple>& cs, std::vector<uint32_t>& pos)
+{
+	const int n = (int)cs.size();
+	pos.assign(n, 0);
+	if (n == 0) return;
+	std::vector<int> idx(n);
+	for (int i = 0; i < n; i++) idx[i] = i;
+	std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return (cs[x].c & 31) < (cs[y].c & 31); });
+	const int G = (n + 31) / 32;
+	std::vector<std::vector<int>> blocks(G);
 	int g = 0;
-	for (int p : idx) {
-		while ((int)groups[g].size() >= (g == G - 1 ? Q - 32 * (G - 1) : 32)) g = (g + 1) % G;
-		groups[g].push_back(p);
+	for (int i : idx) {
+		while ((int)blocks[g].size() >= (g == G - 1 ? n - 32 * (G - 1) : 32)) g = (g + 1) % G;
+		blocks[g].push_back(i);
 		g = (g + 1) % G;
 	}
-	auto cost = [&](const std::vector<int>& grp) {
-		int c1[32] = {0}, c2[32] = {0}, m1 = 0, m2 = 0;
-		for (int p : grp) {
-			const int a = (int)(pairs[2 * p] & 31), b = (int)(pairs[2 * p + 1] & 31);
-			const int f = swapped[p] ? b : a, s2 = swapped[p] ? a : b;
-			m1 = std::max(m1, ++c1[f]);
-			m2 = std::max(m2, ++c2[s2]);
+	auto pb = [&](const Couple& c, bool first) {
+		const int p = first ? c.a : c.b;
+		return (int)((p < 0 ? c.c : partner(pairs, p, c.c)) & 31);
+	};
+	auto cost = [&](const std::vector<int>& blk) {
+		int ca[32] = {0}, cb[32] = {0}, ma = 0, mb = 0;
+		for (int i : blk) {
+			ma = std::max(ma, ++ca[pb(cs[i], true)]);
+			mb = std::max(mb, ++cb[pb(cs[i], false)]);
 		}
-		return m1 + m2;
+		return ma + mb;
 	};
 	for (int gi = 0; gi < G; gi++) {
-		std::vector<int>& grp = groups[gi];
-		int best = cost(grp);
+		std::vector<int>& blk = blocks[gi];
+		int best = cost(blk);
 		for (int pass = 0; pass < 4; pass++) {
 			bool improved = false;
-			for (int p : grp) {
-				swapped[p] ^= 1;
-				const int c = cost(grp);
+			for (int i : blk) {
+				std::swap(cs[i].a, cs[i].b);
+				const int c = cost(blk);
 				if (c < best) { best = c; improved = true; }
-				else swapped[p] ^= 1;
+				else std::swap(cs[i].a, cs[i].b);
 			}
 			if (!improved) break;
 		}
-		for (size_t k = 0; k < grp.size(); k++) pos[grp[k]] = (uint32_t)(32 * gi + k);
+		for (size_t k = 0; k < blk.size(); k++) pos[blk[k]] = (uint32_t)(32 * gi + k);
 	}
 }
 
@@ -169,7 +202,9 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 		}
 	}
 	const int Qs = (int)std_idx.size(), Qg = (int)gen_idx.size();
-	out.npairs2 = (int)pair2_records((uint32_t)Qs);
+	std::vector<Couple> couples;
+	couple_pairs(std_pairs.data(), Qs, N, couples);
+	out.npairs2 = (int)(couples.size() + 31) / 32 * 32;
 	out.ngpairs = Qg;
 	out.off_pairs2 = o; o = align_up(o + (size_t)std::max(out.npairs2, 1) * 64, 16);
 	out.off_gpairs = o; o = align_up(o + (size_t)std::max(Qg, 1) * sizeof(PairRec), 16);
@@ -203,7 +238,7 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 		ends[k] = make_int2(rotbonds[2 * k], rotbonds[2 * k + 1]);
 	}
 	// torsion items in warp-interleaved order (interleave_pos), pairs in
-	// bank-spread groups of 32 (order_pairs)
+	// couples sharing their first atom, in bank-spread blocks (order_couples)
 	uint32_t* it_out = reinterpret_cast<uint32_t*>(B + out.off_tor_items);
 	for (size_t i = 0; i < items.size(); i++) it_out[interleave_pos((uint32_t)i, (uint32_t)items.size())] = items[i];
 	// pair terms in the reference's operand order: desolvation prefactor,
@@ -225,19 +260,24 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 	};
 	float4* pr2 = reinterpret_cast<float4*>(B + out.off_pairs2);
 	for (int r = 0; r < out.npairs2; r++) pair2_pad(pr2, (uint32_t)r, (uint32_t)N);
-	std::vector<uint32_t> ppos;
-	std::vector<uint8_t> pswap;
-	order_pairs(std_pairs.data(), Qs, ppos, pswap);
-	for (int i = 0; i < Qs; i++) {
-		const int p = std_idx[i];
-		uint32_t a1 = pairs[2 * p], a2 = pairs[2 * p + 1];
-		const uint32_t n = kin.VWpars_exp_const[ii.atom_types_const[a1] * (uint32_t)nat + ii.atom_types_const[a2]] & 0xFF;
-		float ac, bd, reqm, dsp, qq, vb;
-		fields(p, ac, bd, reqm, dsp, qq, vb);
-		uint32_t rec, h;
-		pair2_slot(ppos[i], &rec, &h);
-		pair2_set(pr2, rec, h, ac, n == 6 ? bd : 0.0f, n == 10 ? bd : 0.0f, reqm, dp.coeff_desolv * dsp, qq, vb,
-		          pswap[i] ? (a2 | (a1 << 8)) : (a1 | (a2 << 8)));
+	std::vector<uint32_t> slot;
+	order_couples(std_pairs.data(), couples, slot);
+	for (size_t k = 0; k < couples.size(); k++) {
+		const Couple& cp = couples[k];
+		for (uint32_t h = 0; h < 2; h++) {
+			const int q = h ? cp.b : cp.a;                 // index into the AD4 list
+			if (q < 0) {
+				pair2_set(pr2, slot[k], h, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, cp.c | (cp.c << 8));
+				continue;
+			}
+			const int p = std_idx[q];
+			const uint32_t a1 = pairs[2 * p], a2 = pairs[2 * p + 1];
+			const uint32_t n = kin.VWpars_exp_const[ii.atom_types_const[a1] * (uint32_t)nat + ii.atom_types_const[a2]] & 0xFF;
+			float ac, bd, reqm, dsp, qq, vb;
+			fields(p, ac, bd, reqm, dsp, qq, vb);
+			pair2_set(pr2, slot[k], h, ac, n == 6 ? bd : 0.0f, n == 10 ? bd : 0.0f, reqm, dp.coeff_desolv * dsp, qq, vb,
+			          cp.c | (partner(std_pairs.data(), q, cp.c) << 8));
+		}
 	}
 	PairRec* gpr = reinterpret_cast<PairRec*>(B + out.off_gpairs);
 	for (int i = 0; i < Qg; i++) {
@@ -282,6 +322,7 @@ void place_ligand(const PackedLigand& p, const void* dbase, LigDev& L)
 	L.tors_ends = reinterpret_cast<const int2*>(D + p.off_tors_ends);
 	L.tor_items = reinterpret_cast<const uint32_t*>(D + p.off_tor_items);
 	L.npairs2 = p.npairs2; L.ngpairs = p.ngpairs;
+	L.coupled = 1;
 	L.pairs2 = reinterpret_cast<const float4*>(D + p.off_pairs2);
 	L.gpairs = reinterpret_cast<const PairRec*>(D + p.off_gpairs);
 }
