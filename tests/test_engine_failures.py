@@ -114,3 +114,13 @@ def test_stalled_run_times_out_and_the_batch_recovers(grid):
         np.testing.assert_array_equal(r.best_energies, alone[k].best_energies)
         np.testing.assert_array_equal(r.evals, alone[k].evals)
     en.close()
+
+
+@pytest.mark.gpu
+def test_engine_configuration_is_checked():
+    """Out-of-range engine settings are refused at creation."""
+    from adgpu_b200 import engine
+    for kw in ({"priority": 2}, {"priority": -1}, {"threads_per_pose": 48}, {"tick_ms": -1.0},
+               {"idle_timeout_ms": -5.0}):
+        with pytest.raises(lib.AdgpuError):
+            engine.Engine(**kw)
