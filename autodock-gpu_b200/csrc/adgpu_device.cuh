@@ -719,33 +719,42 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	}
 	G.template sum_n<7>(red, true);
 	const float energy = red[6];
-	if (rank == 0 && L.nlig > 0) {
-		// translation (:676-689) and orientation (:695-815) genes
-		S.gg[0] = quant(red[3] * L.spacing);
-		S.gg[1] = quant(red[4] * L.spacing);
-		S.gg[2] = quant(red[5] * L.spacing);
+	if (rank < 3 && L.nlig > 0) {
+		// translation (:676-689) and orientation (:695-815) genes: lane j takes
+		// orientation gene 3 + j (phi, theta, rotation angle) with the same code
+		// on its own angle, and lane 0 also the translation genes; every gene
+		// gets the reference's operations in the reference's order
+		if (rank == 0) {
+			S.gg[0] = quant(red[3] * L.spacing);
+			S.gg[1] = quant(red[4] * L.spacing);
+			S.gg[2] = quant(red[5] * L.spacing);
+		}
 		float tl = norm3df(red[0], red[1], red[2]);
 		float oscale = (tl < kInfinitesimalRadian) ? 1.0f : tl * kInvInfinitesimalRadian;
-		// sin/cos of half the infinitesimal rotation (SIN/COS_HALF_INFINITESIMAL_RADIAN)
-		const float kSinHalfInf = sinf(0.5f * kInfinitesimalRadian), kCosHalfInf = cosf(0.5f * kInfinitesimalRadian);
+		// sin/cos of half the infinitesimal rotation (SIN/COS_HALF_INFINITESIMAL_RADIAN,
+		// common/calcenergy_basic.h:79-80), rounded to float: sin(0.0005) rounds
+		// to 0.0005f, cos(0.0005) to 1 - 2^-23
+		constexpr float kSinHalfInf = 0x1.0624dep-11f, kCosHalfInf = 0x1.fffffcp-1f;
 		float tscale = (tl < kInfinitesimalRadian) ? 0.5f - tl * tl / 48.0f : kSinHalfInf / tl;
 		float4 qt = make_float4(red[0] * tscale, red[1] * tscale, red[2] * tscale,
 		                        (tl < kInfinitesimalRadian) ? 1.0f - tl * tl * 0.125f : kCosHalfInf);
 		float4 tgt = qmul(qt, gr.q);
-		float cur_phi = fmod_pi2(kPiTimes2 + g[3] * kDegToRad);
-		float cur_theta = fmod_pi2(kPiTimes2 + g[4] * kDegToRad);
-		float cur_rot = fmod_pi2(kPiTimes2 + g[5] * kDegToRad);
-		float tgt_rot = 2.0f * fast_acos(tgt.w);
-		float sin_ang = sqrtf(1.0f - tgt.w * tgt.w);
-		float tgt_theta = kPiTimes2 + gr.is_theta_gt_pi * fast_acos(tgt.z / sin_ang);
-		float tgt_phi = fmod_pi2(atan2f(gr.is_theta_gt_pi * tgt.y, gr.is_theta_gt_pi * tgt.x) + kPiTimes2);
-		float gphi = oscale * (fmod_pi2(tgt_phi - cur_phi + kPi) - kPi);
-		float gth = oscale * (fmod_pi2(tgt_theta - cur_theta + kPi) - kPi);
-		float grot = oscale * (fmod_pi2(tgt_rot - cur_rot + kPi) - kPi);
-		float corr = 4.0f * gr.sin_half * gr.sin_half;
-		S.gg[3] = quant(gphi * gr.sin_theta * gr.sin_theta * corr * kDegToRad);
-		S.gg[4] = quant(gth * corr * kDegToRad);
-		S.gg[5] = quant(grot * kDegToRad);
+		// target angle: phi = atan2, theta = 2 pi + sign * acos(z / sin_ang),
+		// rotation = 2 acos(w)
+		float target;
+		if (rank == 0) {
+			target = fmod_pi2(atan2f(gr.is_theta_gt_pi * tgt.y, gr.is_theta_gt_pi * tgt.x) + kPiTimes2);
+		} else {
+			const float sin_ang = sqrtf(1.0f - tgt.w * tgt.w);
+			const float ac = fast_acos(rank == 1 ? tgt.z / sin_ang : tgt.w);
+			target = rank == 1 ? kPiTimes2 + gr.is_theta_gt_pi * ac : 2.0f * ac;
+		}
+		const float cur = fmod_pi2(kPiTimes2 + g[3 + rank] * kDegToRad);
+		float v = oscale * (fmod_pi2(target - cur + kPi) - kPi);
+		const float corr = 4.0f * gr.sin_half * gr.sin_half;
+		if (rank == 0) v = v * gr.sin_theta * gr.sin_theta;
+		if (rank <= 1) v = v * corr;
+		S.gg[3 + rank] = quant(v * kDegToRad);
 	}
 
 	// 6. torsion genes: axis . (r x F) summed over each torsion's rotating atoms (:819-880)
