@@ -707,10 +707,16 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 
 	// 5. torque and total force over the ligand atoms (cuda/calcMergeEneGra.cu:608-661);
 	//    the energy rides along as a seventh sum (one cross-warp exchange, not two)
+	// sizes and pointers of the steps below read once (when L lives in shared
+	// memory, the engine's per-task arguments, the stores to S would otherwise
+	// force reloads in every iteration); not held across the pair loop, whose
+	// register peak would spill
+	const int nlig = L.nlig;
+	const float spacing = L.spacing;
 	float red[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, e_acc};
-	for (int a = rank; a < L.nlig; a += TPP) {
+	for (int a = rank; a < nlig; a += TPP) {
 		const float4 pa = S.xyz[a];
-		float3 r = make_float3((pa.x - gr.mv.x) * L.spacing, (pa.y - gr.mv.y) * L.spacing, (pa.z - gr.mv.z) * L.spacing);
+		float3 r = make_float3((pa.x - gr.mv.x) * spacing, (pa.y - gr.mv.y) * spacing, (pa.z - gr.mv.z) * spacing);
 		const int* fa = S.f3 + 3 * a;
 		float3 f = make_float3(kOneOverTermScale * (float)fa[0], kOneOverTermScale * (float)fa[1], kOneOverTermScale * (float)fa[2]);
 		red[3] += f.x; red[4] += f.y; red[5] += f.z;
@@ -719,15 +725,15 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	}
 	G.template sum_n<7>(red, true);
 	const float energy = red[6];
-	if (rank < 3 && L.nlig > 0) {
+	if (rank < 3 && nlig > 0) {
 		// translation (:676-689) and orientation (:695-815) genes: lane j takes
 		// orientation gene 3 + j (phi, theta, rotation angle) with the same code
 		// on its own angle, and lane 0 also the translation genes; every gene
 		// gets the reference's operations in the reference's order
 		if (rank == 0) {
-			S.gg[0] = quant(red[3] * L.spacing);
-			S.gg[1] = quant(red[4] * L.spacing);
-			S.gg[2] = quant(red[5] * L.spacing);
+			S.gg[0] = quant(red[3] * spacing);
+			S.gg[1] = quant(red[4] * spacing);
+			S.gg[2] = quant(red[5] * spacing);
 		}
 		float tl = norm3df(red[0], red[1], red[2]);
 		float oscale = (tl < kInfinitesimalRadian) ? 1.0f : tl * kInvInfinitesimalRadian;
@@ -758,10 +764,13 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 	}
 
 	// 6. torsion genes: axis . (r x F) summed over each torsion's rotating atoms (:819-880)
-	for (int it = rank; it < L.ntoritems; it += TPP) {
-		uint32_t item = L.tor_items[it];
+	const uint32_t* const tor_items = L.tor_items;
+	const int2* const tors_ends = L.tors_ends;
+	const int ntoritems = L.ntoritems, ngenes = L.ngenes;
+	for (int it = rank; it < ntoritems; it += TPP) {
+		uint32_t item = tor_items[it];
 		int k = item >> 8, la = item & 0xFF;
-		int2 ends = L.tors_ends[k];
+		int2 ends = tors_ends[k];
 		const float4 e0 = S.xyz[ends.x], e1 = S.xyz[ends.y], pl = S.xyz[la];
 		float rx = e0.x, ry = e0.y, rz = e0.z;
 		float ux = e1.x - rx, uy = e1.y - ry, uz = e1.z - rz;
@@ -771,13 +780,13 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 		const int* fl = S.f3 + 3 * la;
 		float3 f = make_float3(kOneOverTermScale * (float)fl[0], kOneOverTermScale * (float)fl[1], kOneOverTermScale * (float)fl[2]);
 		float3 t = cross3(r, f);
-		float on_axis = (ux * t.x + uy * t.y + uz * t.z) * L.spacing;
+		float on_axis = (ux * t.x + uy * t.y + uz * t.z) * spacing;
 		atomicAdd(&S.gg[6 + k], quant(on_axis * kDegToRad));
 	}
 	G.sync();
 	// 7. fixed point -> float, Angstrom/radian scaling of genes >= 3 (:883-899)
-	const float sc = L.spacing * L.spacing * kScAngstromRadian;
-	for (int k = rank; k < L.ngenes; k += TPP) {
+	const float sc = spacing * spacing * kScAngstromRadian;
+	for (int k = rank; k < ngenes; k += TPP) {
 		float v = kOneOverTermScale * (float)S.gg[k];
 		grad[k] = (k >= 3) ? v * sc : v;
 	}
