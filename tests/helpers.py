@@ -115,6 +115,12 @@ def gradient_contract(case: Case, ref: np.ndarray) -> np.ndarray:
     return 1e-4 * np.abs(ref[..., :ng]) + scale * n_terms / 1024.0
 
 
+def oracle_terms(case: Case, genotypes: np.ndarray) -> np.ndarray:
+    """The oracle's eight energy terms per genotype (the seven energy terms
+    and the number of atoms outside the grid), for energy_contract."""
+    return np.array([case.host.score_terms(x)[2] for x in genotypes])
+
+
 def energy_tolerance(ref: np.ndarray) -> np.ndarray:
     """|dE| <= 1e-4 |E| + 1e-6 * |E| floor -> effectively 1e-4 relative with a 1e-3 absolute floor."""
     return 1e-4 * np.abs(ref) + 1e-3
