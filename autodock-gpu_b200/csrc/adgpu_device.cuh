@@ -247,20 +247,46 @@ struct Group {
 	// K <= 8 sums in one pass, each added in the same order as sum() adds a
 	// single value.  scratch_free: the caller has just passed a group barrier
 	// after the scratch's last readers, so the leading barrier is skipped.
+	// Within a warp the values take sum()'s xor butterfly (partners at lane
+	// distance 16, 8, 4, 2, 1) as a reduce-scatter: at distances 16, 8 and 4
+	// a lane keeps half of its values and sends its partner the other half,
+	// so every partial sum is the one sum() forms, and lanes 4k .. 4k+3 end
+	// with value k: 9 shuffles and 9 adds for up to eight values instead of 5
+	// of each per value, then (one warp per group) one shuffle per value to
+	// hand it to every lane.
 	template <int K>
 	__device__ __forceinline__ void sum_n(float* v, bool scratch_free = false) const
 	{
+		static_assert(K >= 1 && K <= 8, "sum_n takes 1 to 8 values");
+		constexpr unsigned kAll = 0xffffffffu;
+		const int lane = rank & 31;
+		const bool h16 = (lane & 16) != 0, h8 = (lane & 8) != 0, h4 = (lane & 4) != 0;
+		float w4[4], w2[2];
 #pragma unroll
-		for (int k = 0; k < K; k++) {
-#pragma unroll
-			for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+		for (int i = 0; i < 4; i++) {
+			const float lo = i < K ? v[i] : 0.0f, hi = 4 + i < K ? v[4 + i] : 0.0f;
+			const float keep = h16 ? hi : lo, send = h16 ? lo : hi;
+			w4[i] = keep + __shfl_xor_sync(kAll, send, 16);
 		}
-		if constexpr (TPP != 32) {
-			const int w = rank >> 5;
-			if (!scratch_free) sync();
-			if ((rank & 31) == 0)
 #pragma unroll
-				for (int k = 0; k < K; k++) red[w * 8 + k] = v[k];
+		for (int i = 0; i < 2; i++) {
+			const float keep = h8 ? w4[2 + i] : w4[i], send = h8 ? w4[i] : w4[2 + i];
+			w2[i] = keep + __shfl_xor_sync(kAll, send, 8);
+		}
+		float w1;
+		{
+			const float keep = h4 ? w2[1] : w2[0], send = h4 ? w2[0] : w2[1];
+			w1 = keep + __shfl_xor_sync(kAll, send, 4);
+		}
+		w1 += __shfl_xor_sync(kAll, w1, 2);
+		w1 += __shfl_xor_sync(kAll, w1, 1);
+		if constexpr (TPP == 32) {
+#pragma unroll
+			for (int k = 0; k < K; k++) v[k] = __shfl_sync(kAll, w1, 4 * k);
+		} else {
+			const int w = rank >> 5, mine = lane >> 2;
+			if (!scratch_free) sync();
+			if ((lane & 3) == 0 && mine < K) red[w * 8 + mine] = w1;
 			sync();
 #pragma unroll
 			for (int k = 0; k < K; k++) {
@@ -270,9 +296,6 @@ struct Group {
 			}
 		}
 	}
-
-	// Six sums in one pass (torque x,y,z and force x,y,z).
-	__device__ __forceinline__ void sum6(float* v) const { sum_n<6>(v); }
 };
 
 // ---- per-pose shared-memory scratch -------------------------------------------------

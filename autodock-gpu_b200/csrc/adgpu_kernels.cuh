@@ -154,12 +154,22 @@ __device__ void gradient_ls_block(const KArgs& a, const PopBufs& pb, uint32_t b,
 	int succ = 0, fail = 0;
 	uint32_t it = 0;
 	const float RHO = 0.8f, EPS = 1e-2f;
+	// ADAM's bias corrections 1 - beta^(it+1): every 32 iterations each lane
+	// computes those of iteration it + lane (the same powf of the same
+	// arguments), and iteration it takes them from lane it % 32, so the
+	// warp runs one powf pair per 32 iterations instead of one per iteration
+	float b1r = 0.f, b2r = 0.f;
 	do {
+		if (METHOD == LS_ADAM && (it & 31u) == 0) {
+			const float t = 1.0f + (float)(it + (uint32_t)(G.rank & 31));
+			b1r = 1.0f - powf(a.dp.adam_beta1, t);
+			b2r = 1.0f - powf(a.dp.adam_beta2, t);
+		}
 		const float energy = score_pose<TPP, true>(a.L, S.gen, S.grad, S.pose, G);
 		float b1p = 0.f, b2p = 0.f;
 		if (METHOD == LS_ADAM) {
-			b1p = 1.0f - powf(a.dp.adam_beta1, 1.0f + (float)it);
-			b2p = 1.0f - powf(a.dp.adam_beta2, 1.0f + (float)it);
+			b1p = __shfl_sync(0xffffffffu, b1r, (int)(it & 31u));
+			b2p = __shfl_sync(0xffffffffu, b2r, (int)(it & 31u));
 		}
 		for (int k = G.rank; k < NG; k += TPP) {
 			float g = S.grad[k];
