@@ -28,6 +28,10 @@ constexpr float kInvPiTimes2 = 1.0f / kPiTimes2;
 constexpr float kTermScale = 1024.0f;
 constexpr float kOneOverTermScale = 1.0f / 1024.0f;
 constexpr float kMaxTerm = 8192.0f;
+// 1.5 * 2^23: a float of magnitude up to 2^22 added to it rounds to an integer
+// (nearest, ties to even) and the sum's bits are kRoundBits + that integer
+constexpr float kRoundMagic = 12582912.0f;
+constexpr uint32_t kRoundBits = 0x4B400000u;
 constexpr float kMaxEnergy = FLT_MAX / 100.0f;
 constexpr float kInfinitesimalRadian = 1E-3f;
 constexpr float kInvInfinitesimalRadian = 1.0f / kInfinitesimalRadian;
@@ -141,6 +145,7 @@ struct LigDev {
 	const float4* pairs2;        // AD4 pairs, two per record (quads, pair2_quad)
 	const PairRec* gpairs;       // pairs with other exponents
 	const float* grid;           // cell records, 32-byte aligned
+	const int* f3_bias;          // with coupled tables: start value of each atom's fixed-point force components (couple_force); nullptr: 0
 };
 
 // ---- math helpers (cuda/calcenergy.cu:31-109) ----------------------------------
@@ -404,14 +409,26 @@ __device__ __forceinline__ void pair_force(int* f3, uint32_t i, uint32_t j, floa
 
 // The fixed-point forces of a couple (pairs A and B sharing atom c, second
 // atoms i and j): c's part of the two is summed in registers and added once.
-__device__ __forceinline__ void couple_force(int* f3, uint32_t c, uint32_t i, uint32_t j, float2 gx, float2 gy, float2 gz)
+// A component is clamped to +-kMaxTerm like quant_scaled and rounded by one
+// packed add of kRoundMagic for both pairs (the same integer as
+// __float2int_rn): its bits are kRoundBits + the quantum.  Atoms i and j
+// take the bits as they are and c minus both, so each add carries a known
+// offset (+kRoundBits for i and j, -2 kRoundBits for c); the integer adds
+// wrap, and every atom's forces start at minus the sum of its offsets over
+// the ligand's records (L.f3_bias, from the tables), so they end exact.
+__device__ __forceinline__ float clamp_term(float v) { return fminf(kMaxTerm, fmaxf(-kMaxTerm, v)); }
+__device__ __forceinline__ void couple_force(unsigned* f3, uint32_t c, uint32_t i, uint32_t j, float2 gx, float2 gy, float2 gz)
 {
-	const int ax = quant_scaled(gx.x), ay = quant_scaled(gy.x), az = quant_scaled(gz.x);
-	const int bx = quant_scaled(gx.y), by = quant_scaled(gy.y), bz = quant_scaled(gz.y);
-	int* fc = f3 + 3 * c;
-	int* fi = f3 + 3 * i;
-	int* fj = f3 + 3 * j;
-	atomicAdd(fc, -ax - bx); atomicAdd(fc + 1, -ay - by); atomicAdd(fc + 2, -az - bz);
+	const float2 mg = f2s(kRoundMagic);
+	const float2 rx = f2add(f2(clamp_term(gx.x), clamp_term(gx.y)), mg);
+	const float2 ry = f2add(f2(clamp_term(gy.x), clamp_term(gy.y)), mg);
+	const float2 rz = f2add(f2(clamp_term(gz.x), clamp_term(gz.y)), mg);
+	const unsigned ax = __float_as_uint(rx.x), ay = __float_as_uint(ry.x), az = __float_as_uint(rz.x);
+	const unsigned bx = __float_as_uint(rx.y), by = __float_as_uint(ry.y), bz = __float_as_uint(rz.y);
+	unsigned* fc = f3 + 3 * c;
+	unsigned* fi = f3 + 3 * i;
+	unsigned* fj = f3 + 3 * j;
+	atomicAdd(fc, 0u - ax - bx); atomicAdd(fc + 1, 0u - ay - by); atomicAdd(fc + 2, 0u - az - bz);
 	atomicAdd(fi, ax); atomicAdd(fi + 1, ay); atomicAdd(fi + 2, az);
 	atomicAdd(fj, bx); atomicAdd(fj + 1, by); atomicAdd(fj + 2, bz);
 }
@@ -515,7 +532,7 @@ __device__ __forceinline__ float pair_loop(const LigDev& L, const PoseSmem& S, i
 			const float2 gdd = f2mul(pg, f2mul(inv_dist, f2s(-kTermScale)));
 			const float2 gx = f2mul(sx, gdd), gy = f2mul(sy, gdd), gz = f2mul(sz, gdd);
 			if constexpr (COUPLED) {
-				couple_force(f3, a1, a2, b2, gx, gy, gz);
+				couple_force(reinterpret_cast<unsigned*>(f3), a1, a2, b2, gx, gy, gz);
 			} else {
 				pair_force(f3, a1, a2, gx.x, gy.x, gz.x);
 				pair_force(f3, b1, b2, gx.y, gy.y, gz.y);
@@ -709,7 +726,12 @@ __device__ float score_pose(const LigDev& L, const float* __restrict__ g, float*
 				}
 			}
 		}
-		if (GRAD) { int* fa = S.f3 + 3 * a; fa[0] = fx; fa[1] = fy; fa[2] = fz; }
+		if (GRAD) {
+			// the start value that cancels couple_force's rounding offsets
+			const unsigned fb = L.f3_bias ? (unsigned)__ldg(L.f3_bias + a) : 0u;
+			int* fa = S.f3 + 3 * a;
+			fa[0] = (int)((unsigned)fx + fb); fa[1] = (int)((unsigned)fy + fb); fa[2] = (int)((unsigned)fz + fb);
+		}
 	}
 	G.sync();
 

@@ -208,6 +208,7 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 	out.ngpairs = Qg;
 	out.off_pairs2 = o; o = align_up(o + (size_t)std::max(out.npairs2, 1) * 64, 16);
 	out.off_gpairs = o; o = align_up(o + (size_t)std::max(Qg, 1) * sizeof(PairRec), 16);
+	out.off_f3_bias = o; o = align_up(o + (size_t)N * 4, 16);
 	out.blob.assign(o, 0);
 	uint8_t* B = out.blob.data();
 
@@ -279,6 +280,24 @@ adgpu_status pack_ligand(const adgpu_dockpars& dp, const adgpu_kc_interintra& ii
 			          cp.c | (partner(std_pairs.data(), q, cp.c) << 8));
 		}
 	}
+	// couple_force adds kRoundBits (mod 2^32) for each record's second atoms
+	// and subtracts it twice for the shared atom, padding included: each atom
+	// starts at minus the sum over the records as the kernel reads them
+	std::vector<int32_t> offsets(N, 0);
+	for (int r = 0; r < out.npairs2; r++) {
+		const float4 q3 = pr2[pair2_quad((uint32_t)r, 3)];
+		uint32_t ija, ijb;
+		std::memcpy(&ija, &q3.z, 4);
+		std::memcpy(&ijb, &q3.w, 4);
+		offsets[ija & 0xFFu] -= 2;
+		offsets[ija >> 8] += 1;
+		offsets[ijb >> 8] += 1;
+	}
+	int32_t* f3b = reinterpret_cast<int32_t*>(B + out.off_f3_bias);
+	for (int a = 0; a < N; a++) {
+		const uint32_t v = 0u - (uint32_t)offsets[a] * kRoundBits;
+		std::memcpy(&f3b[a], &v, 4);
+	}
 	PairRec* gpr = reinterpret_cast<PairRec*>(B + out.off_gpairs);
 	for (int i = 0; i < Qg; i++) {
 		const int p = gen_idx[i];
@@ -325,6 +344,7 @@ void place_ligand(const PackedLigand& p, const void* dbase, LigDev& L)
 	L.coupled = 1;
 	L.pairs2 = reinterpret_cast<const float4*>(D + p.off_pairs2);
 	L.gpairs = reinterpret_cast<const PairRec*>(D + p.off_gpairs);
+	L.f3_bias = reinterpret_cast<const int*>(D + p.off_f3_bias);
 }
 
 void set_grid_fields(LigDev& L, const adgpu_dockpars& dp, const float* cell_grid)

@@ -21,6 +21,7 @@ struct PackedLigand {
 	std::vector<uint8_t> blob;
 	size_t off_atom_xyzq = 0, off_atom_info = 0, off_chain_len = 0, off_chain = 0;
 	size_t off_tors_uv = 0, off_tors_mv = 0, off_tors_ends = 0, off_tor_items = 0, off_pairs2 = 0, off_gpairs = 0;
+	size_t off_f3_bias = 0;           // per-atom start of the fixed-point forces (LigDev::f3_bias)
 	// cost model inputs (algorithmic work per evaluation)
 	long rot_ops = 0;     // torsion rotations + general rotations applied per pose
 };
